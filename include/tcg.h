@@ -1,0 +1,190 @@
+/*
+ * tcg.h -- C-ABI of the B200 operator-application library (libtcg_b200.so).
+ *
+ * The library applies the exchange / transcorrelated operator terms of a
+ * plane-wave HF / TC / BITC calculation to a block of trial orbitals:
+ *
+ *   H2 psi += hf2x psi                         (HF)
+ *   H2 psi += tc2x psi                         (TC, BITC)
+ *   H3 psi += (tc3a1 + tc3b1 + tc3a2a4b2b5 + tc3a3b3b4b6) psi   (TC, BITC)
+ *
+ * It replaces the six routines declared in TC++'s
+ * src/include/calc_hamiltonian.hpp:54-130 (hf2x, tc2x, tc3a1, tc3b1,
+ * tc3a3b3b4b6, tc3a2a4b2b5).  Those take nested
+ * std::vector<...<Eigen::VectorXcd>> containers; here every container is a
+ * flat, packed array of interleaved (re, im) doubles -- the memory layout of
+ * std::complex<double> / Eigen::VectorXcd -- so the reference's C++ host can
+ * pass its buffers after one memcpy per band.
+ *
+ * Conventions (all follow TC++):
+ *  - FFT grid nr[0] x nr[1] x nr[2], x = nr[0] fastest; grid index
+ *    i0 + nr0*(i1 + nr1*i2)  (plane_wave_basis.cpp:205-216, :158-161).
+ *  - Forward FFT (R -> G) is exp(-iGr) scaled by 1/N; backward (G -> R) is
+ *    exp(+iGr) unscaled (plane_wave_basis.cpp:274-289).
+ *  - Orbital coefficients are normalised so that sum_G |c_G|^2 = 1.
+ *  - Vectors k are fractional (crystal) coordinates; Cartesian = recip^T k,
+ *    with recip's rows the reciprocal vectors b_i (bohr^-1, 2pi included,
+ *    crystal_structure.hpp:16).
+ *  - Spin: nspin = num_independent_spins (1 = unpolarised, 2 = polarised).
+ *    density[] always holds two spin channels (bloch_states.hpp).
+ *
+ * Scope: calc_mode "SCF" with every k-point of non-zero weight (the SCF mesh),
+ * no density-matrix mixing (filling_old empty), RPA Jastrow.  In that case
+ * TC++'s sum_of_kVaux vanishes for every k (potentials_coulomb.cpp:186-190),
+ * so the kVaux-weighted divergence corrections of tc2x / tc3a3b3b4b6 /
+ * tc3a2a4b2b5 are identically zero and are not part of this interface.
+ *
+ * Errors: every entry point returns an int status (TCG_OK = 0).  The library
+ * never aborts the process; tcg_last_error() returns a message for the
+ * calling thread's most recent failure.
+ */
+#ifndef TCG_H
+#define TCG_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define TCG_OK               0
+#define TCG_ERR_ARG          1   /* invalid argument / inconsistent sizes        */
+#define TCG_ERR_CUDA         2   /* CUDA runtime error (message has details)     */
+#define TCG_ERR_TIMEOUT      3   /* a bounded device-side wait ran out           */
+#define TCG_ERR_UNSUPPORTED  4   /* valid input outside the implemented scope    */
+#define TCG_ERR_STATE        5   /* call order violated (e.g. apply before set)  */
+#define TCG_ERR_NOMEM        6   /* device allocation failed                     */
+#define TCG_ERR_NUMERIC      7   /* non-finite value detected in an input        */
+
+/* ---- methods / precision --------------------------------------------- */
+#define TCG_METHOD_HF    0
+#define TCG_METHOD_TC    1
+#define TCG_METHOD_BITC  2
+
+#define TCG_PREC_FP64    0   /* complex128 everywhere                          */
+#define TCG_PREC_MIXED   1   /* complex64 FFTs / pair products, FP64 accumulation */
+
+/* ---- term mask ----------------------------------------------------------
+ * Bit i selects one of the reference routines.  hf2x and tc2x add to H2,
+ * the tc3* terms add to H3 (calc_hamiltonian_all.cpp:80-157). */
+#define TCG_TERM_HF2X          (1u << 0)
+#define TCG_TERM_TC2X          (1u << 1)
+#define TCG_TERM_TC3A1         (1u << 2)
+#define TCG_TERM_TC3B1         (1u << 3)
+#define TCG_TERM_TC3A2A4B2B5   (1u << 4)
+#define TCG_TERM_TC3A3B3B4B6   (1u << 5)
+#define TCG_TERMS_HF   (TCG_TERM_HF2X)
+#define TCG_TERMS_TC   (TCG_TERM_TC2X | TCG_TERM_TC3A1 | TCG_TERM_TC3B1 | \
+                        TCG_TERM_TC3A2A4B2B5 | TCG_TERM_TC3A3B3B4B6)
+
+/* ---- static system description (one per run) ----------------------------
+ * "nk_all" below is sum_k nsym_k (Kpoints::num_kpoints_all_scf).  Arrays
+ * indexed by an "all-k" index a list the equivalent k-points irreducible-
+ * major: a = (sum_{k'<ik} nsym_k[k']) + isym, the order of
+ * Kpoints::index_all_kscf (kpoints.cpp:82-91). */
+typedef struct tcg_system_desc {
+    int32_t nr[3];               /* FFT grid (nr1, nr2, nr3)                   */
+    double  recip[9];            /* reciprocal vectors b_i as rows (bohr^-1)   */
+    double  lattice[9];          /* lattice vectors a_i as rows (bohr)         */
+    double  omega;               /* unit-cell volume (bohr^3)                  */
+    int32_t calc_method;         /* TCG_METHOD_*                               */
+    int32_t nspin;               /* num_independent_spins: 1 or 2              */
+    int32_t nk_irr;              /* irreducible SCF k-points                   */
+    int32_t num_kpoints;         /* Kpoints::num_kpoints()                     */
+    const int32_t *nsym_k;       /* [nk_irr] kvectors_scf[ik].size()            */
+    const double  *kvec;         /* [nk_all][3] fractional k                    */
+    const uint8_t *time_rev;     /* [nk_all] is_time_reversal_used_at_k         */
+    const int32_t *rot_index;    /* [nk_all] index_of_rotation_at_k             */
+    int32_t nsymop;              /* Symmetry::num_symmetry_operations           */
+    const int32_t *rotation;     /* [nsymop][3][3] U, row-major, crystal coords */
+    const double  *translation;  /* [nsymop][3] fractional translations         */
+    const int32_t *npw;          /* [nk_irr] num_G_at_k_scf                     */
+    const int32_t *gindex;       /* [nspin][nk_all][npw of its ik] Gindex_at_k_scf */
+    const double  *phase;        /* [nspin][nk_all][npw] complex phase_factor_at_k */
+    double  jastrow_A[4];        /* A_long[s1][s2], row-major (atomic units)   */
+    double  jastrow_F[4];        /* F_long[s1][s2]                              */
+    int32_t includes_div_correction;
+    double  alpha_Vaux;          /* Potentials::alpha_Vaux                      */
+    const double *sum_Vaux;      /* [nk_irr] Potentials::sum_of_Vaux_scf        */
+} tcg_system_desc;
+
+/* ---- per-SCF-iteration state (BlochStates) --------------------------------
+ * phik[s][ik][b] holds num_bands_scf[s] bands of npw[ik] coefficients; the
+ * first nocc[s][ik] carry the occupied orbitals summed over in the exchange
+ * terms, fillings >= 1e-8 enter the divergence corrections (as TC++). */
+typedef struct tcg_state_desc {
+    const int32_t *nbands;       /* [nspin] num_bands_scf                       */
+    const int32_t *nocc;         /* [nspin][nk_irr] num_occupied_bands          */
+    const double  *filling;      /* [nspin][nk_irr][nbands[s]]                  */
+    const double  *phik;         /* [nspin][nk_irr][nbands[s]][npw] complex     */
+    const double  *phik_left;    /* BITC: same layout (left orbitals); else NULL */
+    const double  *density;      /* [2][N] complex, R-space (set_density)       */
+} tcg_state_desc;
+
+/* Opaque context: device copies of the system and state, FFT plans, scratch. */
+typedef struct tcg_ctx tcg_ctx;
+
+/* Create a context on the current CUDA device.  precision = TCG_PREC_*.
+ * Replaces the per-call setup the reference repeats inside every routine
+ * (G-vector tables, Jastrow tables; e.g. calc_hamiltonian_hf2x.cpp:32-37). */
+int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg_ctx **out);
+int tcg_ctx_destroy(tcg_ctx *ctx);
+
+/* Upload the occupied orbitals / fillings / density of one SCF iteration.
+ * BlochStates is const across all calc_hamiltonian::all calls of one
+ * Davidson call (diagonalization_davidson.cpp:228,242,433), so the R-space
+ * occupied orbitals are built once here and reused by every apply. */
+int tcg_set_state(tcg_ctx *ctx, const tcg_state_desc *st);
+
+/* Apply the selected terms to a block of trial orbitals and ACCUMULATE into
+ * h2 / h3 (the reference's "+=" semantics; the caller zeroes them first as
+ * calc_hamiltonian_all.cpp:29-49 does).
+ *   nb_apply : [nspin][nk_irr] bands per (spin, k)  (H2phi[ispin][ik].size())
+ *   psi      : [nspin][nk_irr][nb_apply][npw] complex, packed
+ *   h2, h3   : same layout as psi; h3 may be NULL for HF, h2 NULL if no
+ *              H2 term is selected
+ *   owned    : [nspin][nk_irr][nb_apply] bytes; 0 = band owned by another rank
+ *              (Parallelization::is_assigned_irreducible_kpoints_all_bands);
+ *              NULL = all owned.
+ * Host pointers.  Replaces calc_hamiltonian::hf2x / tc2x / tc3a1 / tc3b1 /
+ * tc3a2a4b2b5 / tc3a3b3b4b6 (calc_hamiltonian.hpp:54-130). */
+int tcg_apply(tcg_ctx *ctx, uint32_t term_mask, const int32_t *nb_apply,
+              const double *psi, double *h2, double *h3, const uint8_t *owned);
+
+/* Same as tcg_apply but psi / h2 / h3 are DEVICE pointers (layout as above)
+ * and the work is queued on the context's stream without a host sync. */
+int tcg_apply_device(tcg_ctx *ctx, uint32_t term_mask, const int32_t *nb_apply,
+                     const void *psi_dev, void *h2_dev, void *h3_dev,
+                     const uint8_t *owned);
+
+/* Divergence-correction scalars for the SCF mesh (Potentials::set_sum_of_Vaux
+ * with set_sum_of_Vaux_each, potentials_coulomb.cpp:60-161), computed on the
+ * device.  Writes alpha_Vaux and sum_Vaux[nk_irr]; needs only the geometry
+ * and k-point fields of sys (sum_Vaux / alpha_Vaux of sys are ignored). */
+int tcg_sum_of_vaux(const tcg_system_desc *sys, double *alpha_out, double *sum_vaux_out);
+
+/* n_s(r) of the given orbitals (BlochStates::set_density, first iteration,
+ * bloch_states_scfloop_filling_density.cpp:256-360), computed on the device;
+ * density_out is [2][N] complex.  Fails with TCG_ERR_NUMERIC if an orbital's
+ * norm <chi|phi> deviates from 1 by more than 1e-4 (as the reference). */
+int tcg_density(tcg_ctx *ctx, const tcg_state_desc *st, double *density_out);
+
+/* Device stream the context queues work on (cudaStream_t, as void*). */
+void *tcg_stream(tcg_ctx *ctx);
+
+/* Number of kernels this context has launched since creation. */
+int64_t tcg_launch_count(const tcg_ctx *ctx);
+
+/* Message of the calling thread's last failure ("" if none). */
+const char *tcg_last_error(void);
+
+/* Library version string. */
+const char *tcg_version(void);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* TCG_H */
