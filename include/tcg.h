@@ -171,6 +171,12 @@ int tcg_sum_of_vaux(const tcg_system_desc *sys, double *alpha_out, double *sum_v
  * norm <chi|phi> deviates from 1 by more than 1e-4 (as the reference). */
 int tcg_density(tcg_ctx *ctx, const tcg_state_desc *st, double *density_out);
 
+/* Tuning knob: bytes of pass temporaries one chunk of (target x source)
+ * pairs may use (0 = default, 1 GiB).  Smaller chunks keep the temporaries
+ * resident in L2; larger ones launch fewer kernels.  No reference
+ * counterpart (TC++ has no chunked pair pipeline). */
+int tcg_set_tuning(tcg_ctx *ctx, int64_t tmp_budget_bytes);
+
 /* Device stream the context queues work on (cudaStream_t, as void*). */
 void *tcg_stream(tcg_ctx *ctx);
 

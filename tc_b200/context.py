@@ -1,0 +1,130 @@
+"""Python host API of the B200 operator library (ctypes over include/tcg.h).
+
+    ctx = Context(system, precision="fp64")   # or "mixed"
+    ctx.set_state(system)                     # once per SCF iteration
+    h2, h3 = ctx.apply(TERMS_TC, psi)         # accumulates like TC++ (H += ...)
+
+There is no CPU path: without the CUDA library or a GPU every call raises
+TCError.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._lib import TCError, check, lib
+
+PRECISIONS = {"fp64": abi.PREC_FP64, "mixed": abi.PREC_MIXED}
+
+
+def _terms(terms):
+    if isinstance(terms, int):
+        return terms
+    if isinstance(terms, str):
+        terms = [terms]
+    m = 0
+    for t in terms:
+        m |= abi.TERM_NAMES[t]
+    return m
+
+
+class Context:
+    def __init__(self, system, precision="fp64", tmp_budget=None):
+        self.system = system
+        self.precision = precision
+        self._sysd, _, self._keep = system.descriptors()
+        h = C.c_void_p()
+        check(lib().tcg_ctx_create(C.byref(self._sysd), PRECISIONS[precision], C.byref(h)))
+        self._h = h
+        if tmp_budget:
+            check(lib().tcg_set_tuning(self._h, int(tmp_budget)))
+        self._state_keep = None
+
+    # -- life cycle ---------------------------------------------------------
+    def close(self):
+        if self._h:
+            lib().tcg_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise TCError(abi.TCG_ERR_STATE, "context closed")
+        return self._h
+
+    @property
+    def launches(self):
+        return int(lib().tcg_launch_count(self.handle))
+
+    @property
+    def stream(self):
+        return lib().tcg_stream(self.handle)
+
+    def set_tuning(self, tmp_budget):
+        check(lib().tcg_set_tuning(self.handle, int(tmp_budget)))
+
+    # -- state ----------------------------------------------------------------
+    def set_state(self, system=None):
+        s = system or self.system
+        _, st, keep = s.descriptors()
+        check(lib().tcg_set_state(self.handle, C.byref(st)))
+        self._state_keep = keep
+
+    def density(self, system=None):
+        s = system or self.system
+        _, st, keep = s.descriptors()
+        st.density = abi.ptr(None, C.c_double)
+        out = np.zeros((2, s.N), dtype=np.complex128)
+        check(lib().tcg_density(self.handle, C.byref(st), out.ctypes.data))
+        return out
+
+    # -- apply ------------------------------------------------------------------
+    def apply(self, terms, psi=None, nb_apply=None, h2=None, h3=None, owned=None):
+        """Host-memory apply; returns (h2, h3) with h += terms(psi)."""
+        s = self.system
+        mask = _terms(terms)
+        nb = np.ascontiguousarray(s.nb_apply if nb_apply is None else nb_apply, dtype=np.int32)
+        psi = np.ascontiguousarray(s.psi if psi is None else psi, dtype=np.complex128)
+        h2 = np.zeros_like(psi) if h2 is None else h2
+        h3 = np.zeros_like(psi) if h3 is None else h3
+        assert h2.dtype == np.complex128 and h2.flags["C_CONTIGUOUS"] and h2.shape == psi.shape
+        assert h3.dtype == np.complex128 and h3.flags["C_CONTIGUOUS"] and h3.shape == psi.shape
+        own = None if owned is None else np.ascontiguousarray(owned, dtype=np.uint8)
+        check(lib().tcg_apply(self.handle, C.c_uint32(mask), nb.ctypes.data_as(C.POINTER(C.c_int32)),
+                              psi.ctypes.data, h2.ctypes.data, h3.ctypes.data,
+                              None if own is None else own.ctypes.data))
+        return h2, h3
+
+    def apply_device(self, terms, psi_ptr, h2_ptr, h3_ptr, nb_apply=None, owned=None):
+        """Device-memory apply on the context's stream (pointers as ints)."""
+        s = self.system
+        nb = np.ascontiguousarray(s.nb_apply if nb_apply is None else nb_apply, dtype=np.int32)
+        own = None if owned is None else np.ascontiguousarray(owned, dtype=np.uint8)
+        check(lib().tcg_apply_device(self.handle, C.c_uint32(_terms(terms)), nb.ctypes.data_as(C.POINTER(C.c_int32)),
+                                     C.c_void_p(psi_ptr), C.c_void_p(h2_ptr), C.c_void_p(h3_ptr),
+                                     None if own is None else own.ctypes.data))
+
+
+def sum_of_vaux(system):
+    """(alpha_Vaux, sum_of_Vaux_scf[nk_irr]) computed on the device."""
+    sysd, _, keep = system.descriptors()
+    alpha = C.c_double()
+    out = np.zeros(system.nk_irr)
+    check(lib().tcg_sum_of_vaux(C.byref(sysd), C.byref(alpha), out.ctypes.data))
+    return alpha.value, out
+
+
+def version():
+    return lib().tcg_version().decode()

@@ -1,0 +1,547 @@
+// api.cu -- C-ABI entry points (include/tcg.h): context life cycle, state
+// upload, the apply orchestration and the host-visible helpers.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <unordered_set>
+#include "ctx.cuh"
+#include "passes.cuh"
+#include "util.cuh"
+#include "terms.cuh"
+
+namespace tcg {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+} // namespace tcg
+
+using namespace tcg;
+
+// ================================================================ C-ABI ====
+extern "C" const char *tcg_last_error(void) { return tcg::g_err; }
+extern "C" const char *tcg_version(void) { return "tcg_b200 0.1 (sm_100a)"; }
+extern "C" void *tcg_stream(tcg_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+extern "C" int64_t tcg_launch_count(const tcg_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+static int validate_system(const tcg_system_desc *s)
+{
+    if (!s) return fail(TCG_ERR_ARG, "null system descriptor");
+    for (int d = 0; d < 3; d++)
+        if (s->nr[d] < 1) return fail(TCG_ERR_ARG, "FFT grid must be positive");
+    if (s->nspin != 1 && s->nspin != 2) return fail(TCG_ERR_ARG, "nspin must be 1 or 2");
+    if (s->calc_method < TCG_METHOD_HF || s->calc_method > TCG_METHOD_BITC) return fail(TCG_ERR_ARG, "bad calc_method");
+    if (s->nk_irr < 1 || s->num_kpoints < 1) return fail(TCG_ERR_ARG, "no k-points");
+    if (!s->nsym_k || !s->kvec || !s->time_rev || !s->npw || !s->gindex || !s->phase)
+        return fail(TCG_ERR_ARG, "missing k-point / G-vector arrays");
+    if (!(s->omega > 0)) return fail(TCG_ERR_ARG, "unit-cell volume must be positive");
+    if (s->includes_div_correction && !s->sum_Vaux) return fail(TCG_ERR_ARG, "sum_Vaux required with div correction");
+    if (s->nsymop < 0) return fail(TCG_ERR_ARG, "negative nsymop");
+    return TCG_OK;
+}
+
+extern "C" int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg_ctx **out)
+{
+    if (!out) return fail(TCG_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    TRY(validate_system(sys));
+    if (precision != TCG_PREC_FP64 && precision != TCG_PREC_MIXED) return fail(TCG_ERR_ARG, "bad precision");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(TCG_ERR_CUDA, "no CUDA device available");
+    }
+    tcg_ctx *c = new tcg_ctx();
+    c->prec = precision;
+    cudaGetDevice(&c->device);
+    Host &h = c->h;
+    for (int d = 0; d < 3; d++) h.n[d] = sys->nr[d];
+    h.N = h.n[0] * h.n[1] * h.n[2];
+    memcpy(h.recip, sys->recip, sizeof h.recip);
+    memcpy(h.lattice, sys->lattice, sizeof h.lattice);
+    h.omega = sys->omega;
+    h.method = sys->calc_method;
+    h.nspin = sys->nspin;
+    h.nk = sys->nk_irr;
+    h.num_kpoints = sys->num_kpoints;
+    h.nsym_k.assign(sys->nsym_k, sys->nsym_k + h.nk);
+    h.npw.assign(sys->npw, sys->npw + h.nk);
+    h.kall_off.assign(h.nk + 1, 0);
+    for (int k = 0; k < h.nk; k++) {
+        if (h.nsym_k[k] < 1) { delete c; return fail(TCG_ERR_ARG, "nsym_k must be >= 1"); }
+        if (h.npw[k] < 1) { delete c; return fail(TCG_ERR_ARG, "npw must be >= 1"); }
+        h.kall_off[k + 1] = h.kall_off[k] + h.nsym_k[k];
+    }
+    h.nk_all = h.kall_off[h.nk];
+    h.ik_of_all.resize(h.nk_all);
+    for (int k = 0; k < h.nk; k++)
+        for (int a = h.kall_off[k]; a < h.kall_off[k + 1]; a++) h.ik_of_all[a] = k;
+    h.kvec.assign(sys->kvec, sys->kvec + 3 * h.nk_all);
+    h.time_rev.assign(sys->time_rev, sys->time_rev + h.nk_all);
+    h.nsymop = sys->nsymop;
+    if (h.nsymop > 0) {
+        if (!sys->rotation || !sys->translation || !sys->rot_index) { delete c; return fail(TCG_ERR_ARG, "missing symmetry arrays"); }
+        h.rotation.assign(sys->rotation, sys->rotation + 9 * h.nsymop);
+        h.translation.assign(sys->translation, sys->translation + 3 * h.nsymop);
+        h.rot_index.assign(sys->rot_index, sys->rot_index + h.nk_all);
+        for (int a = 0; a < h.nk_all; a++)
+            if (h.rot_index[a] < 0 || h.rot_index[a] >= h.nsymop) { delete c; return fail(TCG_ERR_ARG, "rot_index out of range"); }
+    } else {
+        for (int a = 0; a < h.nk_all; a++)
+            if (h.nsym_k[h.ik_of_all[a]] > 1) { delete c; return fail(TCG_ERR_ARG, "symmetry-expanded k-points need rotations"); }
+        h.rotation.assign(9, 0);
+        h.rotation[0] = h.rotation[4] = h.rotation[8] = 1;
+        h.translation.assign(3, 0.0);
+        h.rot_index.assign(h.nk_all, 0);
+        h.nsymop = 1;
+    }
+    memcpy(h.A, sys->jastrow_A, sizeof h.A);
+    memcpy(h.F, sys->jastrow_F, sizeof h.F);
+    h.A_zero = true;
+    for (int i = 0; i < 4; i++)
+        if (fabs(h.A[i]) > 1e-8) h.A_zero = false;
+    if (!h.A_zero)
+        for (int i = 0; i < 4; i++)
+            if (!(fabs(h.F[i]) > 1e-8)) { delete c; return fail(TCG_ERR_ARG, "Jastrow F must be non-zero"); }
+    h.div = sys->includes_div_correction != 0;
+    h.alpha = sys->alpha_Vaux;
+    if (h.div) {
+        h.sum_vaux.assign(sys->sum_Vaux, sys->sum_Vaux + h.nk);
+        if (!(h.alpha > 0)) { delete c; return fail(TCG_ERR_ARG, "alpha_Vaux must be positive"); }
+    } else {
+        h.sum_vaux.assign(h.nk, 0.0);
+    }
+    // SCF mesh check: every k-point must lie on the mesh (kVaux = 0)
+    int rc = TCG_OK;
+    // G maps
+    h.gidx_off.resize((size_t)h.nspin * h.nk_all);
+    size_t off = 0;
+    for (int s = 0; s < h.nspin; s++)
+        for (int a = 0; a < h.nk_all; a++) {
+            h.gidx_off[(size_t)s * h.nk_all + a] = off;
+            off += h.npw[h.ik_of_all[a]];
+        }
+    const size_t ngi = off;
+    std::vector<int> inv((size_t)h.nspin * h.nk_all * h.N, -1);
+    for (int s = 0; s < h.nspin && rc == TCG_OK; s++)
+        for (int a = 0; a < h.nk_all && rc == TCG_OK; a++) {
+            const size_t o = h.gidx_off[(size_t)s * h.nk_all + a];
+            int *im = inv.data() + ((size_t)s * h.nk_all + a) * h.N;
+            for (int p = 0; p < h.npw[h.ik_of_all[a]]; p++) {
+                const int gi = sys->gindex[o + p];
+                if (gi < 0 || gi >= h.N) { rc = fail(TCG_ERR_ARG, "gindex out of range"); break; }
+                if (im[gi] >= 0) { rc = fail(TCG_ERR_ARG, "duplicate gindex within one k-point"); break; }
+                im[gi] = p;
+            }
+        }
+    if (rc != TCG_OK) { delete c; return rc; }
+    // FFT plans
+    GridDesc &g = c->gd;
+    g.n0 = h.n[0]; g.n1 = h.n[1]; g.n2 = h.n[2]; g.N = h.N;
+    for (int d = 0; d < 3; d++)
+        if ((rc = make_axis(h.n[d], g.ax[d])) != TCG_OK) { delete c; return rc; }
+    {
+        const double PI = 3.14159265358979323846;
+        std::vector<double2> t64(3 * MAXN);
+        std::vector<float2> t32(3 * MAXN);
+        for (int d = 0; d < 3; d++)
+            for (int j = 0; j < h.n[d]; j++) {
+                long double a = 2.0L * (long double)PI * j / h.n[d];
+                double cr = (double)cosl(a), ci = -(double)sinl(a);
+                t64[d * MAXN + j] = make_double2(cr, ci);
+                t32[d * MAXN + j] = make_float2((float)cr, (float)ci);
+            }
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            delete c;
+            return fail(TCG_ERR_CUDA, "stream creation failed");
+        }
+        if ((rc = up(c->tw64, t64.data(), t64.size() * sizeof(double2), c->stream)) ||
+            (rc = up(c->tw32, t32.data(), t32.size() * sizeof(float2), c->stream)) ||
+            (rc = up(c->recip, h.recip, sizeof h.recip, c->stream)) ||
+            (rc = up(c->inv, inv.data(), inv.size() * sizeof(int), c->stream)) ||
+            (rc = up(c->phase, sys->phase, ngi * sizeof(double2), c->stream))) {
+            tcg_ctx_destroy(c);
+            return rc;
+        }
+        g.tw64 = c->tw64.as<const double2>();
+        g.tw32 = c->tw32.as<const float2>();
+    }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        tcg_ctx_destroy(c);
+        return fail(TCG_ERR_CUDA, "upload failed");
+    }
+    *out = c;
+    return TCG_OK;
+}
+
+extern "C" int tcg_ctx_destroy(tcg_ctx *c)
+{
+    if (!c) return TCG_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    DBuf *bufs[] = {&c->tw64, &c->tw32, &c->recip, &c->inv, &c->phase, &c->phik, &c->chik, &c->fill,
+                    &c->Rocc, &c->Rchi, &c->Rgrad, &c->dens, &c->occfill, &c->Vloc, &c->dnu, &c->dnuT,
+                    &c->V3a1, &c->V3b1, &c->V3a2, &c->V3b2, &c->Qt, &c->Bt, &c->accP, &c->qtg, &c->div3b6,
+                    &c->psi, &c->h2, &c->h3, &c->Rpsi, &c->Rgpsi, &c->acc2, &c->acc3, &c->qsum, &c->tmp,
+                    &c->tmp2, &c->aux, &c->items, &c->meta};
+    for (DBuf *b : bufs) b->release();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return TCG_OK;
+}
+
+// upload the orbital / filling part of a state (no R-space work)
+static int tcg_set_state_orbitals_only(tcg_ctx *c, const tcg_state_desc *st)
+{
+    if (!c || !st) return fail(TCG_ERR_ARG, "null argument");
+    Host &h = c->h;
+    if (!st->nbands || !st->nocc || !st->filling || !st->phik) return fail(TCG_ERR_ARG, "missing state arrays");
+    const bool bitc = h.method == TCG_METHOD_BITC;
+    if (bitc && !st->phik_left) return fail(TCG_ERR_ARG, "BITC needs phik_left");
+    h.have_state = false;
+    h.nbands.assign(st->nbands, st->nbands + h.nspin);
+    h.nocc.assign(st->nocc, st->nocc + h.nspin * h.nk);
+    size_t nfill = 0;
+    for (int s = 0; s < h.nspin; s++) {
+        if (h.nbands[s] < 0) return fail(TCG_ERR_ARG, "negative nbands");
+        nfill += (size_t)h.nk * h.nbands[s];
+        for (int k = 0; k < h.nk; k++)
+            if (h.nocc[s * h.nk + k] < 0 || h.nocc[s * h.nk + k] > h.nbands[s])
+                return fail(TCG_ERR_ARG, "nocc must lie in [0, nbands]");
+    }
+    h.filling.assign(st->filling, st->filling + nfill);
+    for (double f : h.filling)
+        if (!std::isfinite(f)) return fail(TCG_ERR_NUMERIC, "non-finite filling");
+    h.orb_off.resize((size_t)h.nspin * h.nk);
+    size_t off = 0;
+    for (int s = 0; s < h.nspin; s++)
+        for (int k = 0; k < h.nk; k++) {
+            h.orb_off[(size_t)s * h.nk + k] = off;
+            off += (size_t)h.nbands[s] * h.npw[k];
+        }
+    const size_t norb = off;
+    for (size_t i = 0; i < 2 * norb; i++)
+        if (!std::isfinite(st->phik[i])) return fail(TCG_ERR_NUMERIC, "non-finite orbital coefficient");
+    h.occ_off.resize((size_t)h.nspin * h.nk_all);
+    size_t g = 0;
+    std::vector<double> occfill;
+    for (int s = 0; s < h.nspin; s++)
+        for (int a = 0; a < h.nk_all; a++) {
+            h.occ_off[(size_t)s * h.nk_all + a] = g;
+            const int ik = h.ik_of_all[a];
+            const int no = h.nocc[s * h.nk + ik];
+            for (int i = 0; i < no; i++) {
+                size_t fo = 0;
+                for (int s2 = 0; s2 < s; s2++) fo += (size_t)h.nk * h.nbands[s2];
+                occfill.push_back(h.filling[fo + (size_t)ik * h.nbands[s] + i]);
+            }
+            g += no;
+        }
+    h.nocc_grids = g;
+    int rc;
+    if ((rc = up(c->phik, st->phik, norb * sizeof(double2), c->stream))) return rc;
+    if (bitc && (rc = up(c->chik, st->phik_left, norb * sizeof(double2), c->stream))) return rc;
+    if ((rc = up(c->fill, h.filling.data(), nfill * sizeof(double), c->stream))) return rc;
+    if ((rc = up(c->occfill, occfill.data(), occfill.size() * sizeof(double), c->stream))) return rc;
+    return TCG_OK;
+}
+
+extern "C" int tcg_set_state(tcg_ctx *c, const tcg_state_desc *st)
+{
+    if (st && !st->density) return fail(TCG_ERR_ARG, "missing density");
+    TRY(tcg_set_state_orbitals_only(c, st));
+    Host &h = c->h;
+    int rc;
+    for (size_t i = 0; i < 4 * (size_t)h.N; i++)
+        if (!std::isfinite(st->density[i])) return fail(TCG_ERR_NUMERIC, "non-finite density");
+    if ((rc = up(c->dens, st->density, 2 * (size_t)h.N * sizeof(double2), c->stream))) return rc;
+    rc = c->prec == TCG_PREC_FP64 ? build_occupied<double>(c) : build_occupied<float>(c);
+    if (rc) return rc;
+    rc = c->prec == TCG_PREC_FP64 ? state_terms<double>(c) : state_terms<float>(c);
+    if (rc) return rc;
+    TCG_CUDA(cudaStreamSynchronize(c->stream));
+    h.have_state = true;
+    return TCG_OK;
+}
+
+static int check_apply(tcg_ctx *c, uint32_t mask, const int32_t *nb)
+{
+    if (!c || !nb) return fail(TCG_ERR_ARG, "null argument");
+    if (!c->h.have_state) return fail(TCG_ERR_STATE, "tcg_set_state must be called before tcg_apply");
+    const bool hf = c->h.method == TCG_METHOD_HF;
+    if (mask & ~(TCG_TERMS_HF | TCG_TERMS_TC)) return fail(TCG_ERR_ARG, "unknown term bits");
+    if (hf && (mask & ~TCG_TERMS_HF)) return fail(TCG_ERR_ARG, "TC terms requested for an HF context");
+    if (!hf && (mask & TCG_TERM_HF2X)) return fail(TCG_ERR_ARG, "hf2x requested for a TC/BITC context");
+    for (int i = 0; i < c->h.nspin * c->h.nk; i++)
+        if (nb[i] < 0) return fail(TCG_ERR_ARG, "negative band count");
+    return TCG_OK;
+}
+
+static size_t psi_count(const tcg_ctx *c, const int32_t *nb)
+{
+    size_t n = 0;
+    for (int s = 0; s < c->h.nspin; s++)
+        for (int k = 0; k < c->h.nk; k++) n += (size_t)nb[s * c->h.nk + k] * c->h.npw[k];
+    return n;
+}
+
+extern "C" int tcg_apply_device(tcg_ctx *c, uint32_t mask, const int32_t *nb, const void *psi, void *h2, void *h3,
+                                const uint8_t *owned)
+{
+    TRY(check_apply(c, mask, nb));
+    if (!psi) return fail(TCG_ERR_ARG, "psi is NULL");
+    if ((mask & (TCG_TERM_HF2X | TCG_TERM_TC2X)) && !h2) return fail(TCG_ERR_ARG, "h2 is NULL");
+    if ((mask & ~(TCG_TERM_HF2X | TCG_TERM_TC2X)) && !h3) return fail(TCG_ERR_ARG, "h3 is NULL");
+    ApplyArgs A{};
+    A.mask = mask;
+    A.nb = nb;
+    A.owned = owned;
+    A.psi = (const double2 *)psi;
+    A.h2 = (double2 *)h2;
+    A.h3 = (double2 *)h3;
+    return c->prec == TCG_PREC_FP64 ? apply_impl<double>(c, A) : apply_impl<float>(c, A);
+}
+
+extern "C" int tcg_apply(tcg_ctx *c, uint32_t mask, const int32_t *nb, const double *psi, double *h2, double *h3,
+                         const uint8_t *owned)
+{
+    TRY(check_apply(c, mask, nb));
+    if (!psi) return fail(TCG_ERR_ARG, "psi is NULL");
+    const bool need2 = mask & (TCG_TERM_HF2X | TCG_TERM_TC2X);
+    const bool need3 = mask & ~(TCG_TERM_HF2X | TCG_TERM_TC2X);
+    if (need2 && !h2) return fail(TCG_ERR_ARG, "h2 is NULL");
+    if (need3 && !h3) return fail(TCG_ERR_ARG, "h3 is NULL");
+    const size_t n = psi_count(c, nb);
+    for (size_t i = 0; i < 2 * n; i++)
+        if (!std::isfinite(psi[i])) return fail(TCG_ERR_NUMERIC, "non-finite value in psi");
+    const size_t bytes = n * sizeof(double2);
+    TRY(c->psi.ensure(bytes));
+    TRY(c->h2.ensure(need2 ? bytes : 16));
+    TRY(c->h3.ensure(need3 ? bytes : 16));
+    TCG_CUDA(cudaMemcpyAsync(c->psi.p, psi, bytes, cudaMemcpyHostToDevice, c->stream));
+    if (need2) TCG_CUDA(cudaMemcpyAsync(c->h2.p, h2, bytes, cudaMemcpyHostToDevice, c->stream));
+    if (need3) TCG_CUDA(cudaMemcpyAsync(c->h3.p, h3, bytes, cudaMemcpyHostToDevice, c->stream));
+    TRY(tcg_apply_device(c, mask, nb, c->psi.p, need2 ? c->h2.p : nullptr, need3 ? c->h3.p : nullptr, owned));
+    if (need2) TCG_CUDA(cudaMemcpyAsync(h2, c->h2.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    if (need3) TCG_CUDA(cudaMemcpyAsync(h3, c->h3.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    TCG_CUDA(cudaStreamSynchronize(c->stream));
+    return TCG_OK;
+}
+
+extern "C" int tcg_set_tuning(tcg_ctx *c, int64_t tmp_budget_bytes)
+{
+    if (!c || tmp_budget_bytes < 0) return fail(TCG_ERR_ARG, "bad tuning argument");
+    c->tmp_budget = (size_t)tmp_budget_bytes;
+    return TCG_OK;
+}
+
+// ------------------------------------------------------ divergence sums --
+// one block per (irreducible k, all-k q): shells until the shell sum drops
+// below 1e-20 (potentials_coulomb.cpp:118-139), fixed-tree block reduction.
+__global__ void k_sum_vaux(int nk_all, const double *kirr, const double *kall, RecipC rc, double alpha,
+                           double *partial, int *match, int max_shell)
+{
+    const int ik = blockIdx.x / nk_all, a = blockIdx.x % nk_all;
+    __shared__ double red[256];
+    double kq[3];
+    for (int d = 0; d < 3; d++) {
+        double v = kirr[3 * ik + d] - kall[3 * a + d];
+        while (v < -1e-8) v += 1.0;
+        while (v > 1.0 - 1e-8) v -= 1.0;
+        kq[d] = v;
+    }
+    const bool m = kq[0] * kq[0] + kq[1] * kq[1] + kq[2] * kq[2] < 1e-8;
+    double total = 0.0;
+    if (!m) {
+        double v[3];
+        for (int d = 0; d < 3; d++) v[d] = rc.R[0 * 3 + d] * kq[0] + rc.R[1 * 3 + d] * kq[1] + rc.R[2 * 3 + d] * kq[2];
+        const double k2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        total += exp(-alpha * k2) / k2;
+    }
+    int ns = 1;
+    for (; ns <= max_shell; ns++) {
+        const int w = 2 * ns + 1;
+        double loc = 0.0;
+        for (int i = threadIdx.x; i < w * w * w; i += blockDim.x) {
+            const int gx = i % w - ns, gy = (i / w) % w - ns, gz = i / (w * w) - ns;
+            if (gx != ns && -gx != ns && gy != ns && -gy != ns && gz != ns && -gz != ns) continue;
+            const double x[3] = {kq[0] + gx, kq[1] + gy, kq[2] + gz};
+            double v[3];
+            for (int d = 0; d < 3; d++) v[d] = rc.R[0 * 3 + d] * x[0] + rc.R[1 * 3 + d] * x[1] + rc.R[2 * 3 + d] * x[2];
+            const double g2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+            loc += exp(-alpha * g2) / g2;
+        }
+        red[threadIdx.x] = loc;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+            __syncthreads();
+        }
+        const double shell = red[0];
+        __syncthreads();
+        total += shell;
+        if (shell < 1e-20) break;
+    }
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = total;
+        match[blockIdx.x] = (m ? 1 : 0) | (ns > max_shell ? 2 : 0);
+    }
+}
+
+extern "C" int tcg_sum_of_vaux(const tcg_system_desc *sys, double *alpha_out, double *sum_out)
+{
+    if (!sys || !alpha_out || !sum_out || !sys->nsym_k || !sys->kvec) return fail(TCG_ERR_ARG, "null argument");
+    if (!(sys->omega > 0) || sys->nk_irr < 1) return fail(TCG_ERR_ARG, "bad geometry");
+    const double PI = 3.14159265358979323846;
+    double alpha = cbrt(sys->omega) / (2.0 * PI);
+    alpha = alpha * alpha;
+    const int nk = sys->nk_irr;
+    int nk_all = 0;
+    std::vector<double> kirr(3 * (size_t)nk);
+    for (int k = 0; k < nk; k++) {
+        for (int d = 0; d < 3; d++) kirr[3 * k + d] = sys->kvec[3 * nk_all + d];
+        nk_all += sys->nsym_k[k];
+    }
+    RecipC rc;
+    memcpy(rc.R, sys->recip, sizeof rc.R);
+    DBuf dk, dka, dp, dm;
+    int rc_;
+    if ((rc_ = dk.ensure(kirr.size() * sizeof(double))) || (rc_ = dka.ensure(3 * (size_t)nk_all * sizeof(double))) ||
+        (rc_ = dp.ensure((size_t)nk * nk_all * sizeof(double))) || (rc_ = dm.ensure((size_t)nk * nk_all * sizeof(int))))
+        return rc_;
+    TCG_CUDA(cudaMemcpy(dk.p, kirr.data(), kirr.size() * sizeof(double), cudaMemcpyHostToDevice));
+    TCG_CUDA(cudaMemcpy(dka.p, sys->kvec, 3 * (size_t)nk_all * sizeof(double), cudaMemcpyHostToDevice));
+    k_sum_vaux<<<nk * nk_all, 256>>>(nk_all, dk.as<double>(), dka.as<double>(), rc, alpha, dp.as<double>(), dm.as<int>(), 400);
+    TCG_CUDA(cudaGetLastError());
+    std::vector<double> part((size_t)nk * nk_all);
+    std::vector<int> match((size_t)nk * nk_all);
+    TCG_CUDA(cudaMemcpy(part.data(), dp.p, part.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    TCG_CUDA(cudaMemcpy(match.data(), dm.p, match.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    dk.release(); dka.release(); dp.release(); dm.release();
+    for (int k = 0; k < nk; k++) {
+        double total = 0.0;
+        bool m = false;
+        for (int a = 0; a < nk_all; a++) {
+            const int f = match[(size_t)k * nk_all + a];
+            if (f & 2) return fail(TCG_ERR_NUMERIC, "divergence shell sum did not converge");
+            m = m || (f & 1);
+            total += part[(size_t)k * nk_all + a];
+        }
+        total *= 4.0 * PI;
+        if (m) total -= 4.0 * PI * alpha;
+        sum_out[k] = total;
+    }
+    *alpha_out = alpha;
+    return TCG_OK;
+}
+
+// ---------------------------------------------------------------- density --
+// n_s(r) = sum_{k, isym, i} f |phi(r)|^2  (conj(chi) phi for BITC), /2 when
+// unpolarised (bloch_states_scfloop_filling_density.cpp:282-359)
+__global__ void k_density(int N, int ngrid, const double2 *phi, const double2 *chi, const double *f, double scale,
+                          double2 *out, int bitc)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        double2 acc = {0, 0};
+        for (int gi = 0; gi < ngrid; gi++) {
+            const double2 a = phi[(size_t)gi * N + p];
+            double2 sub;
+            if (bitc) sub = cmulc(chi[(size_t)gi * N + p], a);
+            else sub = {a.x * a.x + a.y * a.y, 0.0};
+            acc = {acc.x + f[gi] * sub.x, acc.y + f[gi] * sub.y};
+        }
+        out[p] = {acc.x * scale, acc.y * scale};
+    }
+}
+__global__ void k_norms(int N, const double2 *phi, const double2 *chi, double2 *norm, int bitc)
+{
+    __shared__ double2 red[256];
+    const int gi = blockIdx.x;
+    double2 loc = {0, 0};
+    for (int p = threadIdx.x; p < N; p += blockDim.x) {
+        const double2 a = phi[(size_t)gi * N + p];
+        const double2 sub = bitc ? cmulc(chi[(size_t)gi * N + p], a) : double2{a.x * a.x + a.y * a.y, 0.0};
+        loc = cadd(loc, sub);
+    }
+    red[threadIdx.x] = loc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] = cadd(red[threadIdx.x], red[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) norm[gi] = red[0];
+}
+
+extern "C" int tcg_density(tcg_ctx *c, const tcg_state_desc *st, double *out)
+{
+    if (!c || !st || !out) return fail(TCG_ERR_ARG, "null argument");
+    TRY(tcg_set_state_orbitals_only(c, st));
+    Host &h = c->h;
+    const size_t N = h.N;
+    const bool bitc = h.method == TCG_METHOD_BITC;
+    // FP64 R-space grids of all occupied orbitals (isym-expanded)
+    DBuf phi, chi, fl, nrm, dn;
+    TRY(phi.ensure(std::max<size_t>(1, h.nocc_grids) * N * sizeof(double2)));
+    if (bitc) TRY(chi.ensure(std::max<size_t>(1, h.nocc_grids) * N * sizeof(double2)));
+    std::vector<SphereItem> items;
+    std::vector<double> f;
+    for (int s = 0; s < h.nspin; s++)
+        for (int a = 0; a < h.nk_all; a++) {
+            const int ik = h.ik_of_all[a];
+            for (int i = 0; i < h.nocc[s * h.nk + ik]; i++) {
+                SphereItem it{};
+                const size_t cof = h.orb_off[(size_t)s * h.nk + ik] + (size_t)i * h.npw[ik];
+                it.coef = c->phik.as<double2>() + cof;
+                it.inv = c->inv.as<int>() + ((size_t)s * h.nk_all + a) * N;
+                it.phase = c->phase.as<double2>() + h.gidx_off[(size_t)s * h.nk_all + a];
+                it.tr = h.time_rev[a];
+                const size_t grid = h.occ_off[(size_t)s * h.nk_all + a] + i;
+                it.out = phi.as<double2>() + grid * N;
+                items.push_back(it);
+                if (bitc) {
+                    it.coef = c->chik.as<double2>() + cof;
+                    it.out = chi.as<double2>() + grid * N;
+                    items.push_back(it);
+                }
+                f.push_back(h.filling[fill_off(h, s, ik) + i]);
+            }
+        }
+    TRY(sphere_to_r<double>(c, items));
+    TRY(fl.ensure(std::max<size_t>(1, f.size()) * sizeof(double)));
+    TRY(nrm.ensure(std::max<size_t>(1, f.size()) * sizeof(double2)));
+    TRY(dn.ensure(2 * N * sizeof(double2)));
+    if (!f.empty()) TCG_CUDA(cudaMemcpyAsync(fl.p, f.data(), f.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const double scale = h.nspin == 1 ? 0.5 : 1.0;
+    for (int s = 0; s < h.nspin; s++) {
+        const size_t g0 = h.occ_off[(size_t)s * h.nk_all];
+        const size_t g1 = s + 1 < h.nspin ? h.occ_off[(size_t)(s + 1) * h.nk_all] : h.nocc_grids;
+        TRY(launch(c, k_density, dim3((unsigned)std::min<size_t>(148 * 8, (N + 255) / 256)), dim3(256), 0, (int)N,
+                   (int)(g1 - g0), (const double2 *)(phi.as<double2>() + g0 * N),
+                   (const double2 *)(bitc ? chi.as<double2>() + g0 * N : nullptr), (const double *)(fl.as<double>() + g0),
+                   scale, dn.as<double2>() + (size_t)s * N, bitc ? 1 : 0));
+    }
+    if (h.nspin == 1)
+        TCG_CUDA(cudaMemcpyAsync(dn.as<double2>() + N, dn.p, N * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+    if (h.nocc_grids)
+        TRY(launch(c, k_norms, dim3((unsigned)h.nocc_grids), dim3(256), 0, (int)N, (const double2 *)phi.as<double2>(),
+                   (const double2 *)(bitc ? chi.as<double2>() : nullptr), nrm.as<double2>(), bitc ? 1 : 0));
+    std::vector<double2> norms(h.nocc_grids);
+    TCG_CUDA(cudaMemcpyAsync(out, dn.p, 2 * N * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    if (h.nocc_grids)
+        TCG_CUDA(cudaMemcpyAsync(norms.data(), nrm.p, h.nocc_grids * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    TCG_CUDA(cudaStreamSynchronize(c->stream));
+    for (const double2 &n : norms) {
+        const double re = n.x / (double)N - 1.0, im = n.y / (double)N;
+        if (std::sqrt(re * re + im * im) > 1e-4) return fail(TCG_ERR_NUMERIC, "normalization breaks");
+    }
+    return TCG_OK;
+}

@@ -1,0 +1,119 @@
+// ctx.cuh -- the library context: device copies of the system / state,
+// FFT plans, scratch arenas, launch helpers.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include <unordered_set>
+#include "../../include/tcg.h"
+#include "fft.cuh"
+
+namespace tcg {
+
+void set_error(const char *fmt, ...);
+
+struct Status {
+    int code = TCG_OK;
+};
+
+#define TCG_CUDA(call)                                                                    \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            tcg::set_error("CUDA error %s at %s:%d (%s)", cudaGetErrorString(e_), __FILE__, \
+                           __LINE__, #call);                                              \
+            return TCG_ERR_CUDA;                                                          \
+        }                                                                                 \
+    } while (0)
+
+// Device buffer (owned).
+struct DBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t b)
+    {
+        if (b <= bytes) return TCG_OK;
+        // kernels queued earlier may still read the old buffer
+        if (p) { cudaDeviceSynchronize(); cudaFree(p); }
+        p = nullptr;
+        bytes = 0;
+        if (b == 0) return TCG_OK;
+        if (cudaMalloc(&p, b) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaMalloc of %zu bytes failed", b);
+            return TCG_ERR_NOMEM;
+        }
+        bytes = b;
+        return TCG_OK;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename X> X *as() const { return reinterpret_cast<X *>(p); }
+};
+
+struct Host {
+    // system
+    int n[3] = {0, 0, 0}, N = 0;
+    double recip[9], lattice[9], omega = 0;
+    int method = 0, nspin = 1, nk = 0, nk_all = 0, num_kpoints = 0;
+    std::vector<int> nsym_k, kall_off, ik_of_all, npw;
+    std::vector<double> kvec;               // [nk_all][3]
+    std::vector<uint8_t> time_rev;
+    std::vector<int> rot_index;
+    int nsymop = 0;
+    std::vector<int> rotation;              // [nsymop][9]
+    std::vector<double> translation;        // [nsymop][3]
+    std::vector<size_t> gidx_off;           // [nspin*nk_all] offset in gindex / phase
+    double A[4], F[4];
+    bool A_zero = true;
+    bool div = false;
+    double alpha = 0;
+    std::vector<double> sum_vaux;
+    // state
+    bool have_state = false;
+    std::vector<int> nbands, nocc;          // [nspin], [nspin][nk]
+    std::vector<double> filling;            // [nspin][nk][nbands]
+    std::vector<size_t> orb_off;            // [nspin*nk] complex offset of band 0
+    std::vector<size_t> occ_off;            // [nspin*nk_all] grid offset into Rocc
+    size_t nocc_grids = 0;
+    bool qp_ready = false;                  // tc3a2a4b2b5 occupied-pair stage done for this state
+};
+
+struct tcg_ctx_impl;
+} // namespace tcg
+
+struct tcg_ctx {
+    int device = 0;
+    int prec = TCG_PREC_FP64;
+    cudaStream_t stream = nullptr;
+    tcg::Host h;
+    tcg::GridDesc gd;
+    // static device data
+    tcg::DBuf tw64, tw32, recip;            // twiddles, reciprocal vectors (9 doubles)
+    tcg::DBuf inv;                          // [nspin][nk_all][N] int32
+    tcg::DBuf phase;                        // [sum npw] double2
+    // state
+    tcg::DBuf phik, chik;                   // G-space fp64 (chik only for BITC)
+    tcg::DBuf fill;                         // [nspin][nk][nbands] doubles
+    tcg::DBuf Rocc, Rchi, Rgrad;            // R-space occupied grids (compute precision)
+    tcg::DBuf dens;                         // [2][N] double2
+    tcg::DBuf occfill;                      // [nocc_grids] doubles: filling of each occupied grid
+    // local three-body potentials built per state
+    tcg::DBuf Vloc;                         // [nspin][N] double2 (tc3a1 + tc3b1 + ...)
+    tcg::DBuf dnu, dnuT;                    // [nspin][3][N] fp64 / compute precision
+    tcg::DBuf V3a1, V3b1, V3a2, V3b2;       // [nspin][N] fp64 local three-body potentials
+    tcg::DBuf Qt, Bt;                       // tc3a2a4b2b5 rotated intermediates [nocc_grids][3][N]
+    tcg::DBuf accP, qtg;                    // occupied-pair accumulators / gathered q2 grids
+    tcg::DBuf div3b6;                       // [nspin][N] fp64 temp_div_3b6 in R space
+    std::vector<double2> t1_3b6;            // [nspin][nk] temp_div_3b6_1
+    // per-apply scratch
+    tcg::DBuf psi, h2, h3;                  // packed fp64
+    tcg::DBuf Rpsi, Rgpsi, acc2, acc3, qsum, tmp, tmp2, aux, items, meta;
+    size_t tmp_budget = 0;                  // bytes per chunk of pass temporaries (0: default 1 GiB)
+    int64_t launches = 0;
+};

@@ -1,0 +1,532 @@
+// terms.cuh -- operator terms on top of the pass kernels.
+//
+//   hf2x         calc_hamiltonian_hf2x.cpp:8-205
+//   tc2x         calc_hamiltonian_tc2x.cpp:11-516   (SCF mesh: kVaux = 0)
+//   tc3a1, tc3b1 calc_hamiltonian_tc3a1.cpp:8-117, tc3b1.cpp:8-135
+//   tc3a3b3b4b6  calc_hamiltonian_tc3a3b3b4b6.cpp:11-863
+//   tc3a2a4b2b5  calc_hamiltonian_tc3a2a4b2b5.cpp:11-1300
+//
+// Every exchange-like sum  sum_{q,i} f_qi X_qi(r) IFFT[K(k-q+G) FFT[Y_qi(r) Z_kj(r)]]
+// runs as chunks of (target bands) x (occupied sources) through the three
+// fused passes (passes.cuh).  All R-space contributions to H2 psi (resp.
+// H3 psi) of one band are summed in one FP64 accumulator and transformed /
+// gathered onto the sphere once at the end.  Work that depends only on the
+// occupied orbitals (R-space orbitals and gradients, the local three-body
+// potentials of tc3a1 / tc3b1 / tc3a2 / tc3b2, and the occupied-pair stage of
+// tc3a2a4b2b5 with its symmetry-rotated intermediates) is done once per
+// tcg_set_state: TC++ recomputes it inside every calc_hamiltonian::all call,
+// although BlochStates is constant across the calls of one Davidson step.
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "ctx.cuh"
+#include "passes.cuh"
+#include "util.cuh"
+#include "jastrow.cuh"
+
+namespace tcg {
+
+struct ApplyArgs {
+    uint32_t mask;
+    const int32_t *nb;
+    const uint8_t *owned;
+    const double2 *psi;
+    double2 *h2, *h3;
+};
+
+constexpr double PI_D = 3.14159265358979323846;
+
+struct RecipC {
+    double R[9];
+};
+
+static inline void cart(const Host &h, const double *x, double *v)
+{
+    for (int d = 0; d < 3; d++) v[d] = h.recip[0 * 3 + d] * x[0] + h.recip[1 * 3 + d] * x[1] + h.recip[2 * 3 + d] * x[2];
+}
+
+__device__ __forceinline__ void gvec(const double *R, const GridDesc &g, int x, int y, int z, const double *q, double *G)
+{
+    const int m0 = miller(x, g.n0), m1 = miller(y, g.n1), m2 = miller(z, g.n2);
+#pragma unroll
+    for (int d = 0; d < 3; d++) G[d] = q[d] + R[0 * 3 + d] * m0 + R[1 * 3 + d] * m1 + R[2 * 3 + d] * m2;
+}
+
+__device__ __forceinline__ void xyz_of(const GridDesc &g, size_t p, int &x, int &y, int &z)
+{
+    x = (int)(p % g.n0);
+    y = (int)((p / g.n0) % g.n1);
+    z = (int)(p / ((size_t)g.n0 * g.n1));
+}
+
+__device__ __forceinline__ void acc_add(double2 *a, double2 v, double f) { *a = {a->x + f * v.x, a->y + f * v.y}; }
+
+// ---------------------------------------------------------------- sphere --
+template <typename T>
+static int sphere_to_r(tcg_ctx *c, const std::vector<SphereItem> &items)
+{
+    using V = typename C2<T>::t;
+    const GridDesc &g = c->gd;
+    if (items.empty()) return TCG_OK;
+    const int nz_tiles = (g.n0 * g.n1 + ZTC - 1) / ZTC;
+    const size_t n = items.size();
+    std::vector<void *> outs(n);
+    for (size_t i = 0; i < n; i++) outs[i] = items[i].out;
+    TRY(c->items.ensure(n * (sizeof(SphereItem) + sizeof(void *))));
+    SphereItem *d_items = c->items.as<SphereItem>();
+    void **d_outs = reinterpret_cast<void **>(d_items + n);
+    TCG_CUDA(cudaMemcpyAsync(d_items, items.data(), n * sizeof(SphereItem), cudaMemcpyHostToDevice, c->stream));
+    TCG_CUDA(cudaMemcpyAsync(d_outs, outs.data(), n * sizeof(void *), cudaMemcpyHostToDevice, c->stream));
+    for (size_t b0 = 0; b0 < n; b0 += 65535) {
+        const unsigned nb = (unsigned)std::min<size_t>(65535, n - b0);
+        TRY(launch(c, k_sphere_z<T>, dim3(nz_tiles, nb), dim3(256), smem_z<V>(g, 0), g,
+                   (const SphereItem *)(d_items + b0), c->recip.as<const double>()));
+        TRY(launch(c, k_xy_inplace<T, +1>, dim3(g.n2, nb), dim3(256), smem_xy<V>(g), g,
+                   (void *const *)(d_outs + b0)));
+    }
+    TCG_CUDA(cudaStreamSynchronize(c->stream));   // c->items is reused by the next caller
+    return TCG_OK;
+}
+
+// In-place full 3D FFT of a list of grids (DIR -1: forward with 1/N).
+template <typename T, int DIR>
+static int fft3_list(tcg_ctx *c, const std::vector<void *> &grids)
+{
+    using V = typename C2<T>::t;
+    const GridDesc &g = c->gd;
+    if (grids.empty()) return TCG_OK;
+    const size_t n = grids.size();
+    TRY(c->items.ensure(n * sizeof(void *)));
+    void **d = c->items.as<void *>();
+    TCG_CUDA(cudaMemcpyAsync(d, grids.data(), n * sizeof(void *), cudaMemcpyHostToDevice, c->stream));
+    const int ntiles = (g.n0 * g.n1 + ZTC - 1) / ZTC;
+    const double scale = DIR < 0 ? 1.0 / (double)g.N : 1.0;
+    for (size_t b0 = 0; b0 < n; b0 += 65535) {
+        const unsigned nb = (unsigned)std::min<size_t>(65535, n - b0);
+        TRY(launch(c, k_xy_inplace<T, DIR>, dim3(g.n2, nb), dim3(256), smem_xy<V>(g), g, (void *const *)(d + b0)));
+        TRY(launch(c, k_z_inplace<T, DIR>, dim3(ntiles, nb), dim3(256), smem_z<V>(g, 0), g, (void *const *)(d + b0),
+                   scale));
+    }
+    TCG_CUDA(cudaStreamSynchronize(c->stream));
+    return TCG_OK;
+}
+
+// --------------------------------------------------------------- targets --
+struct Targets {
+    std::vector<int> s, k, j;
+    std::vector<size_t> psi_off;            // complex offset of the band in psi
+    std::vector<int> blk;                   // block starts (equal (s,k)) + end
+};
+
+static Targets make_targets(const tcg_ctx *c, const ApplyArgs &A)
+{
+    const Host &h = c->h;
+    Targets T;
+    size_t off = 0, flat = 0;
+    for (int s = 0; s < h.nspin; s++)
+        for (int k = 0; k < h.nk; k++) {
+            bool opened = false;
+            for (int j = 0; j < A.nb[s * h.nk + k]; j++, flat++, off += h.npw[k]) {
+                if (A.owned && !A.owned[flat]) continue;
+                if (!opened) { T.blk.push_back((int)T.s.size()); opened = true; }
+                T.s.push_back(s);
+                T.k.push_back(k);
+                T.j.push_back(j);
+                T.psi_off.push_back(off);
+            }
+        }
+    T.blk.push_back((int)T.s.size());
+    return T;
+}
+
+// ============================================================ op plumbing ==
+// Common chunk description shared by the ops: targets tj in [0, nt),
+// sources si in [0, ns), item = tj * ns + si.  Each target belongs to a
+// target block tb (equal k) and each source to a source block sb (equal
+// all-k index); per (tb, sb) a kq vector and a Jastrow table row exist.
+struct ChunkMeta {
+    const int *tb;          // [nt]
+    const int *sb;          // [ns]
+    const double *kq;       // [nTB*nSB][3]
+    const double *tab;      // [nTB*nSB][N][ntab]
+    int nSB, ntab;
+};
+
+template <typename T>
+struct OpBase {
+    using V = typename C2<T>::t;
+    static constexpr bool ZINV = true, REFWD = false;
+    static constexpr int GS = 1;
+    GridDesc g;
+    V *tmp;
+    int nsl;                // tmp slots per item
+    int ns;                 // sources in the chunk
+    ChunkMeta m;
+    RecipC rc;
+    double invN;
+    __device__ V *tmp_grid(int item, int f) const { return tmp + ((size_t)item * nsl + f) * g.N; }
+    __device__ V *zin_grid(int item, int f) const { return tmp_grid(item, f); }
+    __device__ V *out_grid(int item, int o) const { return tmp_grid(item, o); }
+    __device__ V *xyi_grid(int item, int b) const { return tmp_grid(item, b); }
+    __device__ void xyf_begin(int) const {}
+    __device__ void z_begin(int) const {}
+    __device__ void xyi_end(int, int) const {}
+    __device__ int nsrc(int) const { return ns; }
+    __device__ int item_of(int tj, int si) const { return tj * ns + si; }
+    __device__ bool refwd_want(int) const { return false; }
+    __device__ V refwd_load(int, int, int, size_t, V v) const { return v; }
+    __device__ V *refwd_grid(int, int) const { return nullptr; }
+    __device__ V xyf_load(int, int, int, int, int, size_t) const { return czero<V>(); }
+    __device__ int pair_id(int item) const { return m.tb[item / ns] * m.nSB + m.sb[item % ns]; }
+    __device__ const double *kq_of(int item) const { return m.kq + 3 * pair_id(item); }
+    __device__ const double *tab_of(int item) const { return m.tab + (size_t)pair_id(item) * g.N * m.ntab; }
+};
+
+// =================================================================== hf2x ==
+template <typename T>
+struct OpHF2X : OpBase<T> {
+    using V = typename C2<T>::t;
+    static constexpr int NF = 1, NB = 1;
+    const V *Rpsi, *Rocc;     // chunk's first target / source
+    double2 *acc;
+    const double *fill;
+    __device__ V xyf_load(int item, int, int, int, int, size_t p) const
+    {
+        const int tj = item / this->ns, si = item % this->ns;
+        return cmulc(Rocc[(size_t)si * this->g.N + p], Rpsi[(size_t)tj * this->g.N + p]);
+    }
+    __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
+    {
+        double G[3];
+        gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
+        const double t = G[0] * G[0] + G[1] * G[1] + G[2] * G[2];
+        const double v = t < 1e-8 ? 0.0 : this->invN / t;   // 1/|k-q+G|^2 (hf2x.cpp:93-104), 1/N folded in
+        return cscale(in[0], (decltype(in[0].x))v);
+    }
+    __device__ void xyi_accum(int tj, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        acc_add(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], Rocc[(size_t)si * this->g.N + p])), fill[si]);
+    }
+};
+
+// =================================================================== tc2x ==
+template <typename T>
+struct OpTC2X : OpBase<T> {
+    using V = typename C2<T>::t;
+    static constexpr int NF = 4, NB = 4;
+    const V *Rpsi, *Rgpsi;        // [nt][N], [nt][3][N]
+    const V *Rocc, *Rchi, *Rgrad; // [ns][N], [ns][N], [ns][3][N]
+    double2 *acc;
+    const double *fill;
+    __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
+    {
+        const size_t N = this->g.N;
+        const int tj = item / this->ns, si = item % this->ns;
+        const V chi = Rchi[(size_t)si * N + p];
+        const V rhs = f == 0 ? Rpsi[(size_t)tj * N + p] : Rgpsi[((size_t)tj * 3 + (f - 1)) * N + p];
+        return cmulc(chi, rhs);     // tc2x.cpp:350, :374
+    }
+    __device__ V zmix(int item, int o, int x, int y, int z, const V *in) const
+    {
+        using S = decltype(in[0].x);
+        double G[3];
+        gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
+        const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
+        const double *tab = this->tab_of(item);
+        const double u = tab[2 * p + 1] * this->invN;
+        if (o == 0) {   // [2a_x] rho V_2body + [2b_x2] sum_d rho_d du_d   (tc2x.cpp:378-386)
+            V r = cscale(in[0], (S)(tab[2 * p] * this->invN));
+#pragma unroll
+            for (int d = 0; d < 3; d++) r = cadd(r, cscale(in[1 + d], (S)(G[d] * u)));
+            return r;
+        }
+        return cscale(in[0], (S)(G[o - 1] * u));   // [2b_x1] rho du_d (tc2x.cpp:354-358)
+    }
+    __device__ void xyi_accum(int tj, int item, int b, size_t p, const V *v) const
+    {
+        const size_t N = this->g.N;
+        const int si = item % this->ns;
+        const V o = b == 0 ? Rocc[(size_t)si * N + p] : Rgrad[((size_t)si * 3 + (b - 1)) * N + p];
+        acc_add(acc + (size_t)tj * N + p, to64(cmul(v[0], o)), b == 0 ? fill[si] : -fill[si]);
+    }
+};
+
+// Jastrow tables per (tb, sb): modes select the columns
+enum TabMode { TAB_TC2X = 0, TAB_U_SX = 1, TAB_U_SS = 2, TAB_U_QX = 3 };
+// TAB_TC2X : [V_2body(s,s), u(s,s)]                         (tc2x.cpp:266-276)
+// TAB_U_SX : [u(G; 0, s), u(G; 1, s)]                        (tc3a3b3b4b6.cpp:208-217)
+// TAB_U_SS : [u(G; s, s)]                                    (tc3a3b3b4b6.cpp:679-686)
+// TAB_U_QX : [u(G; s, 0), u(G; s, 1)]                        (tc3a2a4b2b5.cpp:244-253)
+__global__ void k_tables(GridDesc g, RecipC rc, Jastrow J, int mode, int s, int npair, const double *kq, double *tab)
+{
+    const int ntab = mode == TAB_U_SS ? 1 : 2;
+    const size_t total = (size_t)npair * g.N;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int pr = (int)(i / g.N);
+        const size_t p = i % g.N;
+        int x, y, z;
+        xyz_of(g, p, x, y, z);
+        double G[3];
+        gvec(rc.R, g, x, y, z, kq + 3 * pr, G);
+        double *o = tab + i * ntab;
+        if (mode == TAB_TC2X) { o[0] = J.tc2body(G, s, s); o[1] = J.uk(G, s, s); }
+        else if (mode == TAB_U_SX) { o[0] = J.uk(G, 0, s); o[1] = J.uk(G, 1, s); }
+        else if (mode == TAB_U_SS) { o[0] = J.uk(G, s, s); }
+        else { o[0] = J.uk(G, s, 0); o[1] = J.uk(G, s, 1); }
+    }
+}
+
+// ======================================================= tc3a3b3b4b6 ops ==
+// stage A: first q loop (tc3a3b3b4b6.cpp:192-368)
+template <typename T>
+struct OpTC3A : OpBase<T> {
+    using V = typename C2<T>::t;
+    static constexpr int NF = 4, NB = 7;
+    static constexpr bool REFWD = true;
+    const V *Rpsi, *Rocc, *Rchi;  // [nt][N], [ns][N]
+    const V *dnu;                 // [3][N] of the targets' spin
+    const double2 *dens;          // [2][N]
+    double2 *acc, *qsum;          // [nt][N], [nt][3][N]
+    const double *fill;
+    V *tmp2;                      // [items][6][N]
+    int s;
+    double b3;
+    __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
+    {
+        const size_t N = this->g.N;
+        const int tj = item / this->ns, si = item % this->ns;
+        const V chi = Rchi[(size_t)si * N + p];
+        V rhs = Rpsi[(size_t)tj * N + p];
+        if (f > 0) rhs = cmul(dnu[(size_t)(f - 1) * N + p], rhs);   // dnu_phi (:236)
+        return cmulc(chi, rhs);
+    }
+    __device__ V zmix(int item, int o, int x, int y, int z, const V *in) const
+    {
+        using S = decltype(in[0].x);
+        double G[3];
+        gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
+        const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
+        const double *tab = this->tab_of(item) + 2 * p;
+        if (o == 0) {   // [3b3] sum_d du[s]_d FFT(dnu_phi_d conj chi) (:286-295)
+            const double u = tab[s] * this->invN;
+            V r = cscale(in[1], (S)(G[0] * u));
+            r = cadd(r, cscale(in[2], (S)(G[1] * u)));
+            return cadd(r, cscale(in[3], (S)(G[2] * u)));
+        }
+        const int xs = (o - 1) / 3, d = (o - 1) % 3;   // phiphi f du[xs]_d (:306-314)
+        const double f = fill[item % this->ns];
+        return cscale(in[0], (S)(f * G[d] * tab[xs] * this->invN));
+    }
+    __device__ void xyi_accum(int tj, int item, int b, size_t p, const V *v) const
+    {
+        const size_t N = this->g.N;
+        const int si = item % this->ns;
+        const V phq = Rocc[(size_t)si * N + p];
+        if (b == 0) {
+            acc_add(acc + (size_t)tj * N + p, to64(cmul(v[0], phq)), fill[si] * b3);
+        } else {
+            const int xs = (b - 1) / 3, d = (b - 1) % 3;
+            if (xs == s) acc_add(qsum + ((size_t)tj * 3 + d) * N + p, to64(cmul(v[0], phq)), 1.0);
+        }
+    }
+    __device__ bool refwd_want(int b) const { return b > 0; }
+    __device__ V refwd_load(int, int, int b, size_t p, V v) const
+    {
+        const int xs = (b - 1) / 3;
+        return cmul(v, from64<V>(dens[(size_t)xs * this->g.N + p]));   // orbital * n_s2 (:332)
+    }
+    __device__ V *refwd_grid(int item, int b) const { return tmp2 + ((size_t)item * 6 + (b - 1)) * this->g.N; }
+};
+
+// stage B: [3b6] sum_{s2,d} FFT(.) du[s2]_d -> IFFT x phi_q (:333-348)
+template <typename T>
+struct OpTC3B : OpBase<T> {
+    using V = typename C2<T>::t;
+    static constexpr int NF = 6, NB = 1;
+    const V *Rocc;
+    double2 *acc;
+    V *tmp2;
+    double b6;
+    __device__ V *zin_grid(int item, int f) const { return tmp2 + ((size_t)item * 6 + f) * this->g.N; }
+    __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
+    {
+        using S = decltype(in[0].x);
+        double G[3];
+        gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
+        const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
+        const double *tab = this->tab_of(item) + 2 * p;
+        V r = czero<V>();
+#pragma unroll
+        for (int xs = 0; xs < 2; xs++)
+#pragma unroll
+            for (int d = 0; d < 3; d++) r = cadd(r, cscale(in[3 * xs + d], (S)(G[d] * tab[xs] * this->invN)));
+        return r;
+    }
+    __device__ void xyi_accum(int tj, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        acc_add(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], Rocc[(size_t)si * this->g.N + p])), b6);
+    }
+};
+
+// stage C: [3b4] second q loop (:664-767)
+template <typename T>
+struct OpTC3C : OpBase<T> {
+    using V = typename C2<T>::t;
+    static constexpr int NF = 3, NB = 1;
+    const V *Rocc, *Rchi;
+    const double2 *qsum;      // [nt][3][N]
+    double2 *acc;
+    const double *fill;
+    double b4;
+    __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
+    {
+        const size_t N = this->g.N;
+        const int tj = item / this->ns, si = item % this->ns;
+        return cmulc(Rchi[(size_t)si * N + p], from64<V>(qsum[((size_t)tj * 3 + f) * N + p]));
+    }
+    __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
+    {
+        using S = decltype(in[0].x);
+        double G[3];
+        gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
+        const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
+        const double u = this->tab_of(item)[p] * this->invN;
+        V r = cscale(in[0], (S)(G[0] * u));
+        r = cadd(r, cscale(in[1], (S)(G[1] * u)));
+        return cadd(r, cscale(in[2], (S)(G[2] * u)));
+    }
+    __device__ void xyi_accum(int tj, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        acc_add(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], Rocc[(size_t)si * this->g.N + p])), b4 * fill[si]);
+    }
+};
+
+// ======================================================= tc3a2a4b2b5 ops ==
+// occupied-pair stage (tc3a2a4b2b5.cpp:210-443): targets (q2, i2), sources (q1, i1)
+template <typename T, bool BITC>
+struct OpQP : OpBase<T> {
+    using V = typename C2<T>::t;
+    static constexpr int NF = BITC ? 2 : 1, NB = BITC ? 12 : 6, GS = BITC ? 2 : 1;
+    const V *Rq2, *Rq2c;          // targets phi_q2(r), chi_q2(r)  [nt][N]
+    const V *Rocc, *Rchi;         // sources phi_q1, chi_q1        [ns][N]
+    double2 *acc;                 // [nt][nacc][N]: 3a2[nspin], 3a4[3], 3b5[3]
+    const double *fill;           // sources
+    int nacc, nspin, sq;
+    __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
+    {
+        const size_t N = this->g.N;
+        const int tj = item / this->ns, si = item % this->ns;
+        if (f == 0) return cmulc(Rchi[(size_t)si * N + p], Rq2[(size_t)tj * N + p]);   // (:359)
+        return cmulc(Rocc[(size_t)si * N + p], Rq2c[(size_t)tj * N + p]);              // (:365)
+    }
+    __device__ V zmix(int item, int o, int x, int y, int z, const V *in) const
+    {
+        using S = decltype(in[0].x);
+        double G[3];
+        gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
+        const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
+        const double *tab = this->tab_of(item) + 2 * p;
+        int xs, d, w;
+        if (BITC) { w = o & 1; xs = (o >> 1) / 3; d = (o >> 1) % 3; }
+        else { w = 0; xs = o / 3; d = o % 3; }
+        return cscale(in[w], (S)(G[d] * tab[xs] * this->invN));   // du[x]_d * phiphi (:378, :385)
+    }
+    __device__ void xyi_accum(int tj, int item, int b, size_t p, const V *v) const
+    {
+        const size_t N = this->g.N;
+        const int si = item % this->ns;
+        const double f1 = fill[si];
+        int xs, d;
+        if (BITC) { xs = (b >> 1) / 3; d = (b >> 1) % 3; }
+        else { xs = b / 3; d = b % 3; }
+        const int xr = nspin == 1 ? 0 : xs;
+        double2 *A = acc + (size_t)tj * nacc * N;
+        const double2 o1 = to64(v[0]);
+        if (BITC) {
+            const double2 o2 = to64(v[1]);
+            acc_add(A + (size_t)xr * N + p, cmulc(o2, o1), -f1);                  // -f1 orbital conj(orbital2)
+            if (xs == sq) {
+                acc_add(A + (size_t)(nspin + d) * N + p, to64(cmul(v[0], Rocc[(size_t)si * N + p])), f1);
+                const double2 cc = to64(cmul(cconj(v[1]), cconj(Rchi[(size_t)si * N + p])));
+                acc_add(A + (size_t)(nspin + 3 + d) * N + p, cc, -f1);               // (:428-430)
+            }
+        } else {
+            acc_add(A + (size_t)xr * N + p, double2{o1.x * o1.x + o1.y * o1.y, 0.0}, -f1);   // (:404-406)
+            if (xs == sq) acc_add(A + (size_t)(nspin + d) * N + p, to64(cmul(v[0], Rocc[(size_t)si * N + p])), f1);
+        }
+    }
+};
+
+// forward transform of pair products (3a2 divergence correction, :544-550)
+template <typename T>
+struct OpPairFwd : OpBase<T> {
+    using V = typename C2<T>::t;
+    static constexpr int NF = 2, NB = 2;
+    static constexpr bool ZINV = false;
+    const V *A0, *B0, *A1, *B1;   // item i: conj(A0_i) B0_i, conj(A1_i) B1_i, pointers per item via strides
+    const int *ia0, *ib0, *ia1, *ib1;   // per item grid indices; results: tmp slots 0, 1 (G space)
+    __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
+    {
+        const size_t N = this->g.N;
+        if (f == 0) return cmulc(A0[(size_t)ia0[item] * N + p], B0[(size_t)ib0[item] * N + p]);
+        return cmulc(A1[(size_t)ia1[item] * N + p], B1[(size_t)ib1[item] * N + p]);
+    }
+    __device__ V zmix(int, int o, int, int, int, const V *in) const
+    {
+        return cscale(in[o], (decltype(in[0].x))this->invN);
+    }
+    __device__ void xyi_accum(int, int, int, size_t, const V *) const {}
+};
+
+// band part of 3a4 / 3b5 (:848-911): targets (k, j), sources (q2sym, i2)
+template <typename T>
+struct OpBand : OpBase<T> {
+    using V = typename C2<T>::t;
+    static constexpr int NF = 4, NB = 4;
+    const V *Rpsi;                // [nt][N]
+    const V *Rocc, *Rchi;         // phi_q2sym, chi_q2sym [ns][N]
+    const V *Qt, *Bt;             // rotated intermediates [ns][3][N]
+    double2 *acc;
+    const double *fill;           // f2 per source
+    double fa4, fb5;
+    __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
+    {
+        const size_t N = this->g.N;
+        const int tj = item / this->ns, si = item % this->ns;
+        const V phj = Rpsi[(size_t)tj * N + p];
+        if (f == 0) return cmulc(Rchi[(size_t)si * N + p], phj);   // (:865)
+        return cmul(Bt[((size_t)si * 3 + (f - 1)) * N + p], phj);   // (:885)
+    }
+    __device__ V zmix(int item, int o, int x, int y, int z, const V *in) const
+    {
+        using S = decltype(in[0].x);
+        double G[3];
+        gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
+        const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
+        const double u = this->tab_of(item)[p] * this->invN;
+        if (o < 3) {    // f2 a4 phiphi du0_d  (:867-872)
+            const double f2 = fill[item % this->ns];
+            return cscale(in[0], (S)(f2 * fa4 * G[o] * u));
+        }
+        V r = cscale(in[1], (S)(G[0] * u));     // sum_d FFT(Bt_d phi_j) du0_d (:882-890)
+        r = cadd(r, cscale(in[2], (S)(G[1] * u)));
+        return cadd(r, cscale(in[3], (S)(G[2] * u)));
+    }
+    __device__ void xyi_accum(int tj, int item, int b, size_t p, const V *v) const
+    {
+        const size_t N = this->g.N;
+        const int si = item % this->ns;
+        double2 *a = acc + (size_t)tj * N + p;
+        if (b < 3) acc_add(a, to64(cmul(Qt[((size_t)si * 3 + b) * N + p], v[0])), 1.0);    // (:875)
+        else acc_add(a, to64(cmul(v[0], Rocc[(size_t)si * N + p])), fb5 * fill[si]);      // (:894)
+    }
+};
+
+} // namespace tcg
+
+#include "tc3.cuh"

@@ -1,0 +1,75 @@
+// util.cuh -- error helpers, kernel launch wrapper, upload helper.
+#pragma once
+#include <mutex>
+#include <unordered_set>
+#include "ctx.cuh"
+#include "passes.cuh"
+
+namespace tcg {
+
+inline int fail(int code, const char *msg)
+{
+    set_error("%s", msg);
+    return code;
+}
+
+// ---------------------------------------------------------------- plans --
+inline int make_axis(int n, Axis &ax)
+{
+    if (n < 1 || n > MAXN) return fail(TCG_ERR_UNSUPPORTED, "FFT axis length outside 1..128");
+    ax.n = n;
+    ax.nst = 0;
+    int m = n;
+    while (m % 8 == 0 && ax.nst < MAXST) { ax.R[ax.nst++] = 8; m /= 8; }
+    while (m % 4 == 0 && ax.nst < MAXST) { ax.R[ax.nst++] = 4; m /= 4; }
+    while (m % 2 == 0 && ax.nst < MAXST) { ax.R[ax.nst++] = 2; m /= 2; }
+    for (int q = 3; m > 1 && ax.nst < MAXST; q += 2)
+        while (m % q == 0 && ax.nst < MAXST) {
+            if (q > 16) return fail(TCG_ERR_UNSUPPORTED, "FFT axis length has a prime factor > 16");
+            ax.R[ax.nst++] = q;
+            m /= q;
+        }
+    if (m != 1) return fail(TCG_ERR_UNSUPPORTED, "FFT axis length not factorisable");
+    return TCG_OK;
+}
+
+// smem sizes (bytes) of the pass kernels
+template <typename V> inline size_t smem_xy(const GridDesc &g) { return sizeof(V) * (3 * MAXN + 2 * (size_t)g.n0 * g.n1); }
+template <typename V> inline size_t smem_z(const GridDesc &g, int nf) { return sizeof(V) * (3 * MAXN + (size_t)(nf + 2) * ZTC * g.n2); }
+
+// Launch with the dynamic-smem attribute set once per kernel.
+inline std::mutex g_attr_mu;
+inline std::unordered_set<const void *> g_attr_set;
+template <typename K, typename... Args>
+inline int launch(tcg_ctx *c, K kernel, dim3 grid, dim3 block, size_t smem, Args... args)
+{
+    if (grid.x == 0 || grid.y == 0 || grid.z == 0) return TCG_OK;
+    if (smem > 48 * 1024) {
+        std::lock_guard<std::mutex> lk(g_attr_mu);
+        if (!g_attr_set.count((const void *)kernel)) {
+            TCG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+            g_attr_set.insert((const void *)kernel);
+        }
+    }
+    if (smem > 227 * 1024) return fail(TCG_ERR_UNSUPPORTED, "kernel shared memory exceeds 227 KB");
+    kernel<<<grid, block, smem, c->stream>>>(args...);
+    c->launches++;
+    TCG_CUDA(cudaGetLastError());
+    return TCG_OK;
+}
+
+#define TRY(x)                     \
+    do {                           \
+        int rc_ = (x);             \
+        if (rc_ != TCG_OK) return rc_; \
+    } while (0)
+
+inline int up(DBuf &b, const void *src, size_t bytes, cudaStream_t s)
+{
+    TRY(b.ensure(bytes));
+    if (bytes) TCG_CUDA(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, s));
+    return TCG_OK;
+}
+
+
+} // namespace tcg
