@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Benchmark of the BITC H psi operator apply on B200.
+
+Workload (default): the batched BITC configuration -- fcc Si a=10.26 bohr,
+4x4x4 Monkhorst-Pack mesh (64 k), 1/2|k+G|^2 < 14 Ha (645-692 plane waves
+per k), FFT grid 36^3, 16 bands per k (4 occupied), independent seeded left
+and right orbitals, RPA Jastrow A=0.5 F=1.2.  Seeded synthetic inputs
+(tc_b200.synth); no dataset is involved.
+
+One step = all per-state work (R-space occupied orbitals and gradients,
+local three-body potentials, the occupied-pair stage of tc3a2a4b2b5) plus
+the apply of tc2x + tc3a1 + tc3b1 + tc3a2a4b2b5 + tc3a3b3b4b6 to all 1024
+(k, band) trial orbitals, i.e. what calc_hamiltonian::all computes for the
+two- and three-body exchange terms.  Metric: band-applies per second
+(1024 per step), mixed precision (complex64 FFTs, FP64 accumulation);
+the FP64 form is measured alongside and |dE| between them reported.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BITC H psi band-applies/s, mixed vs FP64 on one B200 at |dE|<=1e-6 Ha"
+UNIT = "band-applies/s"
+TERMS = ["tc2x", "tc3a1", "tc3b1", "tc3a2a4b2b5", "tc3a3b3b4b6"]
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return FALLBACK_PEAKS, "fallback"
+
+
+# ------------------------------------------------------------ clocks ----
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------ distributed -----
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def shard_owned(system, world, rank):
+    """Band-applies sharded over ranks by k-point, round robin
+    (Parallelization::set_orbital_parallelization splits (spin, k, band)
+    blocks, parallelization.cpp:127-172)."""
+    flags = []
+    for s in range(system.nspin):
+        for k in range(system.nk_irr):
+            own = (k % world) == rank
+            flags += [1 if own else 0] * int(system.nb_apply[s][k])
+    return np.array(flags, dtype=np.uint8)
+
+
+# ---------------------------------------------------------- FFT model ---
+def fft_model(system):
+    """Algorithmic 3D-FFT count of one step (recomputation removed):
+    per band-apply (8 tc2x + 22 tc3a3b3b4b6 + 10 tc3a2a4b2b5) N_k N_o + 6,
+    plus 14 (BITC) or 7 (TC) per occupied pair and ~10 per occupied orbital."""
+    nk = system.num_kpoints
+    no = int(system.nocc[0][0])
+    nb = int(system.nb_apply.sum())
+    per_band = (8 + 22 + 10) * nk * no + 6
+    pair = 14 if system.method == "BITC" else 7
+    shared = pair * (nk * no) ** 2 + 10 * nk * no
+    return per_band * nb + shared
+
+
+# ---------------------------------------------------------------- ours --
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from tc_b200 import abi, synth
+    from tc_b200.context import Context
+
+    world, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    system = synth.config(args.config)
+    nb_total = int(system.nb_apply.sum())
+    owned = shard_owned(system, world, rank) if world > 1 else None
+    mask = abi.TERMS_TC if system.method != "HF" else abi.TERMS_HF
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    psi_dev = torch.from_numpy(system.psi.view(np.float64)).to(dev)
+    n2 = psi_dev.numel()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MiB > 126 MB L2
+
+    def device_arm(prec, steps, warmup, profile=False):
+        ctx = Context(system, prec, tmp_budget=args.tmp_budget)
+        ctx.set_state()
+        h2 = torch.zeros(n2, dtype=torch.float64, device=dev)
+        h3 = torch.zeros(n2, dtype=torch.float64, device=dev)
+        stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+
+        def step():
+            h2.zero_()
+            h3.zero_()
+            torch.cuda.synchronize()
+            ctx.refresh_state()
+            ctx.apply_device(mask, psi_dev.data_ptr(), h2.data_ptr(), h3.data_ptr(), owned=owned)
+
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        barrier()
+        times = []
+        l0 = ctx.launches
+        clocks = ClockSampler(local)
+        clocks.start()
+        for _ in range(steps):
+            flush.fill_(1.0)           # L2 flush between timed iterations (outside the events)
+            torch.cuda.synchronize()
+            h2.zero_()
+            h3.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.refresh_state()
+            ctx.apply_device(mask, psi_dev.data_ptr(), h2.data_ptr(), h3.data_ptr(), owned=owned)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+        clk = clocks.stop()
+        barrier()
+        launches = ctx.launches - l0
+        prof = None
+        if profile:
+            ctx.profile(True)
+            step()
+            torch.cuda.synchronize()
+            prof = ctx.profile_read()
+            ctx.profile(False)
+        res = dict(times=times, launches=launches, clocks=clk, prof=prof,
+                   h2=h2.cpu().numpy().view(np.complex128), h3=h3.cpu().numpy().view(np.complex128))
+        ctx.close()
+        return res
+
+    mixed = device_arm("mixed", args.steps, args.warmup, profile=True)
+    t_mixed = max_over_ranks(sum(mixed["times"]))
+    fp64 = None
+    if not args.no_fp64:
+        fp64 = device_arm("fp64", max(1, args.fp64_steps), 1)
+        t_fp64 = max_over_ranks(sum(fp64["times"]))
+
+    # ---- end to end through the C-ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        import torch as T_
+        pin = {}
+        for name in ("psi", "phik", "phik_left"):
+            arr = getattr(system, name)
+            if arr is None:
+                continue
+            t = T_.empty(arr.size * 2, dtype=T_.float64, pin_memory=True)
+            v = t.numpy().view(np.complex128)
+            v[:] = arr
+            pin[name] = t
+            setattr(system, name, v)
+        dens_t = T_.empty(system.density.size * 2, dtype=T_.float64, pin_memory=True)
+        dv = dens_t.numpy().view(np.complex128).reshape(system.density.shape)
+        dv[:] = system.density
+        system.density = dv
+        h2p = T_.zeros(n2, dtype=T_.float64, pin_memory=True).numpy().view(np.complex128)
+        h3p = T_.zeros(n2, dtype=T_.float64, pin_memory=True).numpy().view(np.complex128)
+        ctx = Context(system, "mixed", tmp_budget=args.tmp_budget)
+        for _ in range(1):
+            ctx.set_state()
+            ctx.apply(mask, h2=h2p, h3=h3p, owned=owned)
+        barrier()
+        et = []
+        for _ in range(args.steps):
+            h2p[:] = 0
+            h3p[:] = 0
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.set_state()
+            ctx.apply(mask, h2=h2p, h3=h3p, owned=owned)
+            torch.cuda.synchronize()
+            et.append(time.perf_counter() - t0)
+        ctx.close()
+        t_e2e = max_over_ranks(sum(et))
+        state_bytes = system.phik.nbytes + (system.phik_left.nbytes if system.phik_left is not None else 0) \
+            + system.density.nbytes + system.filling.nbytes
+        e2e = {"value": nb_total * args.steps / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": int(state_bytes + 3 * system.psi.nbytes),
+               "d2h_bytes_per_step": int(2 * system.psi.nbytes)}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    # ---- energies and |dE| (mixed vs FP64)
+    e_mixed = system.energy_terms(mixed["h2"], mixed["h3"])
+    dE = None
+    if fp64 is not None:
+        e_fp64 = system.energy_terms(fp64["h2"], fp64["h3"])
+        dE = abs(sum(e_mixed) - sum(e_fp64))
+    value = nb_total * args.steps / t_mixed
+    pk, pk_kind = peaks()
+    # ---- roofline of the dominant kernel (pass tag with the most device time)
+    prof = mixed["prof"] or {}
+    dom = max(((t, v) for t, v in prof.items() if t != "misc"), key=lambda x: x[1][1], default=None)
+    roof = None
+    if dom is not None:
+        tag, (cnt, ms, by) = dom
+        achieved = by / (ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": f"pass:{tag}", "achieved": round(achieved, 1),
+                "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
+                "peak_kind": pk_kind, "launches": cnt, "avg_launch_ms": round(ms / cnt, 4),
+                "traffic": traffic_for(args.config, tag)}
+    nfft = fft_model(system)
+    step_s = t_mixed / args.steps
+    step_roof = {"fft_count": nfft, "bytes_model": nfft * 2 * system.N * 8,
+                 "achieved_gbs": round(nfft * 2 * system.N * 8 / step_s / 1e9, 1),
+                 "frac": round(nfft * 2 * system.N * 8 / step_s / 1e9 / pk["hbm_gbs"], 4)}
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(step_s * 1e3, 2), "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "c64-fft/f64-acc", "data": "synthetic (seeded)",
+        "config": {"workload": "BITC batched apply: fcc Si a=10.26, 4x4x4 MP (64 k), 14 Ha (645-692 PW/k), "
+                               "grid 36^3, 16 bands/k (4 occ), all 5 TC terms + per-state work",
+                   "config": args.config, "band_applies_per_step": nb_total, "parallelism": f"k-shard{world}",
+                   "l2": "flushed between timed steps (256 MiB write)"},
+        "fp64": None if fp64 is None else {"value": round(nb_total * len(fp64["times"]) / t_fp64, 3),
+                                           "ms_per_step": round(t_fp64 / len(fp64["times"]) * 1e3, 2)},
+        "mixed_over_fp64": None if fp64 is None else round((nb_total * args.steps / t_mixed) /
+                                                           (nb_total * len(fp64["times"]) / t_fp64), 3),
+        "dE_mixed_vs_fp64_Ha": dE,
+        "energy": {"E2": [e_mixed[0].real, e_mixed[0].imag], "E3": [e_mixed[1].real, e_mixed[1].imag]},
+        "roofline": roof,
+        "roofline_step": step_roof,
+        "e2e": e2e,
+        "gpu_launches": mixed["launches"],
+        "clocks": mixed["clocks"],
+        "profile": {t: {"launches": v[0], "ms": round(v[1], 3), "alg_GB": round(v[2] / 1e9, 3)} for t, v in prof.items()},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(system, args.cpu_qstride)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def traffic_for(config, tag):
+    """DRAM bytes per launch of the dominant pass kernel from the committed
+    ncu summary (profiles/traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    try:
+        d = json.load(open(p))
+        return d.get(config, {}).get(tag)
+    except (OSError, ValueError):
+        return None
+
+
+# ------------------------------------------------------- CPU baseline ---
+def cpu_baseline(system, qstride, threads=None):
+    """Oracle (CPU restatement, OpenMP) timed on a bounded sample of the
+    same workload: one band-apply per host thread and every qstride-th
+    source k-point in the q-sums, extrapolated to the full apply (per-band
+    work x qstride x bands/sample, occupied-pair stage x qstride^2)."""
+    from tc_b200 import abi
+    from oracle import oracle as O
+    if threads:
+        O.set_threads(threads)
+    nth = O.threads()
+    nb = int(system.nb_apply.sum())
+    own = np.zeros(nb, dtype=np.uint8)
+    own[(np.arange(min(nth, nb)) * nb) // min(nth, nb)] = 1
+    O.set_qstride(qstride)
+    O.reset_timers()
+    t0 = time.perf_counter()
+    O.apply(system, abi.TERMS_TC if system.method != "HF" else abi.TERMS_HF, owned=own)
+    wall = time.perf_counter() - t0
+    sh, tot, ini = O.timers()
+    O.set_qstride(1)
+    full = (tot - sh - ini) * qstride * (nb / own.sum()) + sh * qstride ** 2 + ini
+    return {"value": nb / full, "unit": UNIT, "cores": nth, "kind": "port",
+            "sample": f"CPU restatement of TC++ arithmetic (not the reference binary), {int(own.sum())} band-applies, "
+                      f"q-sums over every {qstride}-th k-point, {wall:.1f} s wall, extrapolated to the full apply "
+                      f"({full:.0f} s)", "cpu_model": cpu_model()}
+
+
+def cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args):
+    """Reference arm: TC++'s own path cannot be built here (MPI, FFTW3,
+    Eigen3, Boost absent), so the CPU restatement of its arithmetic (the
+    oracle) is timed on the host cores, a bounded sample per step."""
+    world, rank, _ = dist_info()
+    if rank != 0:
+        return
+    from tc_b200 import synth
+    system = synth.config(args.config)
+    for _ in range(args.warmup and 1):
+        pass   # the oracle has no warm-up state; one sample per step below
+    vals, samples = [], []
+    for _ in range(args.steps):
+        cb = cpu_baseline(system, args.ref_qstride)
+        vals.append(cb["value"])
+        samples.append(cb)
+    v = statistics.median(vals)
+    cb = dict(samples[-1])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "BITC batched apply, same as the GPU arm", "config": args.config},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="C3")
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-qstride", type=int, default=8)
+    ap.add_argument("--ref-qstride", type=int, default=16)
+    ap.add_argument("--tmp-budget", type=int, default=0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("note: warmup raised to 3 (timing rule)", file=sys.stderr)
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -138,6 +138,12 @@ int tcg_ctx_destroy(tcg_ctx *ctx);
  * occupied orbitals are built once here and reused by every apply. */
 int tcg_set_state(tcg_ctx *ctx, const tcg_state_desc *st);
 
+/* Redo the per-state work of the last tcg_set_state from the device-resident
+ * copy (R-space orbitals, local three-body potentials, and -- on the next
+ * apply -- the tc3a2a4b2b5 occupied-pair stage), without a host upload.
+ * Equivalent to calling tcg_set_state again with the same arrays. */
+int tcg_refresh_state(tcg_ctx *ctx);
+
 /* Apply the selected terms to a block of trial orbitals and ACCUMULATE into
  * h2 / h3 (the reference's "+=" semantics; the caller zeroes them first as
  * calc_hamiltonian_all.cpp:29-49 does).
@@ -176,6 +182,16 @@ int tcg_density(tcg_ctx *ctx, const tcg_state_desc *st, double *density_out);
  * resident in L2; larger ones launch fewer kernels.  No reference
  * counterpart (TC++ has no chunked pair pipeline). */
 int tcg_set_tuning(tcg_ctx *ctx, int64_t tmp_budget_bytes);
+
+/* Per-kernel timing with CUDA events recorded on the context stream around
+ * every launch (off by default; enabling clears earlier records).  No
+ * reference counterpart (TC++ times whole phases at 1 s resolution,
+ * my_clock.cpp:19-33). */
+int tcg_profile(tcg_ctx *ctx, int enable);
+/* Aggregate of the recorded launches per pass tag ("xyf", "z", "xyi",
+ * "misc"): count, device milliseconds and algorithmic bytes (N s per grid
+ * and pass; a 3D FFT = 2 N s).  tags: cap x 16 chars. */
+int tcg_profile_read(tcg_ctx *ctx, int cap, char *tags, int64_t *count, double *ms, double *bytes, int *ntags);
 
 /* Device stream the context queues work on (cudaStream_t, as void*). */
 void *tcg_stream(tcg_ctx *ctx);

@@ -41,6 +41,8 @@ def lib():
         L.tco_last_error.restype = C.c_char_p
         L.tco_set_threads.argtypes = [C.c_int]
         L.tco_get_threads.restype = C.c_int
+        L.tco_set_qstride.argtypes = [C.c_int]
+        L.tco_timers.argtypes = [C.POINTER(C.c_double)] * 3
         _lib = L
     return _lib
 
@@ -105,3 +107,18 @@ def tc2body(sysm, G, s1, s2):
     sysd, st, keep = sysm.descriptors()
     g = (C.c_double * 3)(*[float(x) for x in G])
     return lib().tco_tc2body(C.byref(sysd), g, s1, s2)
+
+
+def set_qstride(s):
+    lib().tco_set_qstride(int(s))
+
+
+def timers():
+    """(shared occupied-pair stage, total, set-up) seconds since reset."""
+    a, b, d = C.c_double(), C.c_double(), C.c_double()
+    lib().tco_timers(C.byref(a), C.byref(b), C.byref(d))
+    return a.value, b.value, d.value
+
+
+def reset_timers():
+    lib().tco_reset_timers()

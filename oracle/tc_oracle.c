@@ -33,6 +33,29 @@ static const double PI = 3.14159265358979323846;
 
 static __thread char g_err[512];
 static int g_threads = 0;
+/* Timing-sample mode for the CPU baseline: q-loops over the all-k sources
+ * visit only every g_qstride-th k-point (the results are then partial sums,
+ * used for timing only); g_t_shared accumulates the wall time of the
+ * occupied-pair stage of tc3a2a4b2b5, g_t_total of tco_apply. */
+static int g_qstride = 1;
+static double g_t_shared = 0.0, g_t_total = 0.0, g_t_init = 0.0;
+static double now_s(void)
+{
+#ifdef _OPENMP
+    return omp_get_wtime();
+#else
+    return 0.0;
+#endif
+}
+void tco_set_qstride(int s) { g_qstride = s > 0 ? s : 1; }
+void tco_timers(double *shared, double *total, double *init)
+{
+    if (shared) *shared = g_t_shared;
+    if (total) *total = g_t_total;
+    if (init) *init = g_t_init;
+}
+void tco_reset_timers(void) { g_t_shared = g_t_total = g_t_init = 0.0; }
+#define QSKIP(a) ((a) % g_qstride != 0)
 
 static int fail(int code, const char *fmt, ...)
 {
@@ -460,7 +483,7 @@ static void run_hf2x(const octx *c, const packing *P, const task *T, int nt, con
         fft3_exec(&c->F, phij, 0);
         for (int a = 0; a < c->nk_all; a++) {
             const int iq = c->ik_of_all[a];
-            if (nocc(c, s, iq) == 0) continue;
+            if (nocc(c, s, iq) == 0 || QSKIP(a)) continue;
             double dk[3], kq[3];
             for (int d = 0; d < 3; d++) dk[d] = kref[d] - c->sys->kvec[3 * a + d];
             cart(c->sys, dk, kq);
@@ -547,7 +570,7 @@ static void run_tc2x(const octx *c, const packing *P, const task *T, int nt, con
         fft3_exec(&c->F, phij, 0);
         for (int a = 0; a < c->nk_all; a++) {
             const int iq = c->ik_of_all[a];
-            if (nocc(c, s, iq) == 0) continue;
+            if (nocc(c, s, iq) == 0 || QSKIP(a)) continue;
             double qv[3], kq[3];
             cart(c->sys, c->sys->kvec + 3 * a, qv);
             for (int d = 0; d < 3; d++) kq[d] = kvect[d] - qv[d];
@@ -766,7 +789,7 @@ static void run_tc3a3b3b4b6(const octx *c, const packing *P, const task *T, int 
         /* first q loop: 3b3, 3b6, qsum for 3a3 / 3b4 (:192-368) */
         for (int a = 0; a < c->nk_all; a++) {
             const int iq = c->ik_of_all[a];
-            if (nocc(c, s, iq) == 0) continue;
+            if (nocc(c, s, iq) == 0 || QSKIP(a)) continue;
             double qv[3], kq[3];
             cart(c->sys, c->sys->kvec + 3 * a, qv);
             for (int d = 0; d < 3; d++) kq[d] = kvect[d] - qv[d];
@@ -866,7 +889,7 @@ static void run_tc3a3b3b4b6(const octx *c, const packing *P, const task *T, int 
         memset(Hsub, 0, sizeof(cplx) * N);
         for (int a = 0; a < c->nk_all; a++) {
             const int iq = c->ik_of_all[a];
-            if (nocc(c, s, iq) == 0) continue;
+            if (nocc(c, s, iq) == 0 || QSKIP(a)) continue;
             double qv[3], kq[3];
             cart(c->sys, c->sys->kvec + 3 * a, qv);
             for (int d = 0; d < 3; d++) kq[d] = kvect[d] - qv[d];
@@ -986,7 +1009,8 @@ static void run_tc3a2a4b2b5(const octx *c, const packing *P, const task *T, int 
         for (int d = 0; d < 3; d++) qsum3b2[d] = gnew(c);
         for (int iq2 = 0; iq2 < c->nk; iq2++) {
             const int no2 = nocc(c, sq, iq2);
-            if (no2 == 0) continue;
+            if (no2 == 0 || QSKIP(iq2)) continue;
+            const double t_sh0 = now_s();
             double q2v[3];
             cart(c->sys, c->sys->kvec + 3 * a0(c, iq2), q2v);
             /* occupied-pair stage (:210-443): accumulators per (i2, part) */
@@ -1009,7 +1033,7 @@ static void run_tc3a2a4b2b5(const octx *c, const packing *P, const task *T, int 
                         for (int d = 0; d < 3; d++) du[x][d] = malloc(sizeof(double) * N);
                     for (int a1 = abeg; a1 < aend; a1++) {
                         const int iq1 = c->ik_of_all[a1];
-                        if (nocc(c, sq, iq1) == 0) continue;
+                        if (nocc(c, sq, iq1) == 0 || QSKIP(a1)) continue;
                         double q1v[3], qq[3];
                         cart(c->sys, c->sys->kvec + 3 * a1, q1v);
                         for (int d = 0; d < 3; d++) qq[d] = q2v[d] - q1v[d];
@@ -1058,6 +1082,7 @@ static void run_tc3a2a4b2b5(const octx *c, const packing *P, const task *T, int 
                     for (int x = 0; x < 2; x++)
                         for (int d = 0; d < 3; d++) free(du[x][d]);
                 }
+            g_t_shared += now_s() - t_sh0;
             /* reduce parts in fixed order into part 0 */
             for (int i2 = 0; i2 < no2; i2++) {
                 cplx *A0 = acc + ((size_t)i2 * nparts) * nacc * N;
@@ -1244,9 +1269,11 @@ int tco_apply(const tcg_system_desc *sys, const tcg_state_desc *st, uint32_t mas
     if ((mask & ~(TCG_TERM_HF2X | TCG_TERM_TC2X)) && !h3) return fail(TCG_ERR_ARG, "h3 is NULL");
     if (sys->nsymop > 0 && (!sys->rotation || !sys->translation || !sys->rot_index))
         return fail(TCG_ERR_ARG, "missing symmetry arrays");
+    const double t0 = now_s();
     octx c;
     rc = ctx_init(&c, sys, st, 1);
     if (rc) { ctx_free(&c); return rc; }
+    g_t_init += now_s() - t0;
     packing P;
     pack_init(&P, &c, nb_apply);
     task *T;
@@ -1261,6 +1288,7 @@ int tco_apply(const tcg_system_desc *sys, const tcg_state_desc *st, uint32_t mas
     free(T);
     free(P.off);
     ctx_free(&c);
+    g_t_total += now_s() - t0;
     return TCG_OK;
 }
 

@@ -50,6 +50,14 @@ int tco_sum_of_vaux(const tcg_system_desc *sys, double *alpha_out, double *sum_v
 void tco_set_threads(int n);
 int tco_get_threads(void);
 
+/* Timing-sample mode (CPU baseline only): visit every s-th source k-point
+ * in the q-sums (results become partial sums); timers of the shared
+ * occupied-pair stage, of whole tco_apply calls and of their set-up
+ * (R-space occupied orbitals), in seconds. */
+void tco_set_qstride(int s);
+void tco_timers(double *shared, double *total, double *init);
+void tco_reset_timers(void);
+
 const char *tco_last_error(void);
 
 #ifdef __cplusplus

@@ -39,6 +39,10 @@ def lib():
         L.tcg_last_error.restype = C.c_char_p
         L.tcg_version.restype = C.c_char_p
         L.tcg_set_tuning.argtypes = [vp, C.c_int64]
+        L.tcg_profile.argtypes = [vp, C.c_int]
+        L.tcg_profile_read.argtypes = [vp, C.c_int, C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        L.tcg_refresh_state.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -50,4 +54,4 @@ def check(rc):
 
 EXPORTS = ["tcg_ctx_create", "tcg_ctx_destroy", "tcg_set_state", "tcg_apply", "tcg_apply_device",
            "tcg_sum_of_vaux", "tcg_density", "tcg_stream", "tcg_launch_count", "tcg_last_error",
-           "tcg_version", "tcg_set_tuning"]
+           "tcg_version", "tcg_set_tuning", "tcg_profile", "tcg_profile_read", "tcg_refresh_state"]

@@ -82,6 +82,27 @@ class Context:
         check(lib().tcg_set_state(self.handle, C.byref(st)))
         self._state_keep = keep
 
+    def refresh_state(self):
+        check(lib().tcg_refresh_state(self.handle))
+
+    def profile(self, enable=True):
+        check(lib().tcg_profile(self.handle, 1 if enable else 0))
+
+    def profile_read(self):
+        """{tag: (launches, device ms, algorithmic bytes)} of recorded launches."""
+        cap = 16
+        tags = C.create_string_buffer(16 * cap)
+        cnt = (C.c_int64 * cap)()
+        ms = (C.c_double * cap)()
+        by = (C.c_double * cap)()
+        n = C.c_int()
+        check(lib().tcg_profile_read(self.handle, cap, tags, cnt, ms, by, C.byref(n)))
+        out = {}
+        for i in range(n.value):
+            t = tags.raw[16 * i:16 * i + 16].split(b"\0")[0].decode()
+            out[t] = (int(cnt[i]), float(ms[i]), float(by[i]))
+        return out
+
     def density(self, system=None):
         s = system or self.system
         _, st, keep = s.descriptors()

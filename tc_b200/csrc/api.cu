@@ -273,6 +273,21 @@ extern "C" int tcg_set_state(tcg_ctx *c, const tcg_state_desc *st)
     return TCG_OK;
 }
 
+// Redo all per-state work (R-space occupied orbitals and gradients, local
+// three-body potentials; the tc3a2a4b2b5 occupied-pair stage on the next
+// apply) from the device-resident state of the last tcg_set_state.
+extern "C" int tcg_refresh_state(tcg_ctx *c)
+{
+    if (!c) return fail(TCG_ERR_ARG, "null context");
+    if (!c->h.have_state) return fail(TCG_ERR_STATE, "no state to refresh");
+    int rc = c->prec == TCG_PREC_FP64 ? build_occupied<double>(c) : build_occupied<float>(c);
+    if (rc) return rc;
+    rc = c->prec == TCG_PREC_FP64 ? state_terms<double>(c) : state_terms<float>(c);
+    if (rc) return rc;
+    TCG_CUDA(cudaStreamSynchronize(c->stream));
+    return TCG_OK;
+}
+
 static int check_apply(tcg_ctx *c, uint32_t mask, const int32_t *nb)
 {
     if (!c || !nb) return fail(TCG_ERR_ARG, "null argument");
@@ -543,5 +558,48 @@ extern "C" int tcg_density(tcg_ctx *c, const tcg_state_desc *st, double *out)
         const double re = n.x / (double)N - 1.0, im = n.y / (double)N;
         if (std::sqrt(re * re + im * im) > 1e-4) return fail(TCG_ERR_NUMERIC, "normalization breaks");
     }
+    return TCG_OK;
+}
+
+// ------------------------------------------------------------- profiling --
+extern "C" int tcg_profile(tcg_ctx *c, int enable)
+{
+    if (!c) return fail(TCG_ERR_ARG, "null context");
+    for (auto &r : c->prof_recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    c->prof_recs.clear();
+    c->prof = enable != 0;
+    return TCG_OK;
+}
+
+// Aggregate the recorded launches per tag: for tag i writes count, total
+// device milliseconds and algorithmic bytes.  Returns the number of tags via
+// *ntags (<= cap).  Tags: "xyf", "z", "xyi", "misc".
+extern "C" int tcg_profile_read(tcg_ctx *c, int cap, char *tags /* cap x 16 */, int64_t *count, double *ms,
+                                double *bytes, int *ntags)
+{
+    if (!c || !ntags) return fail(TCG_ERR_ARG, "null argument");
+    TCG_CUDA(cudaStreamSynchronize(c->stream));
+    std::vector<std::string> names;
+    std::vector<int64_t> cnt;
+    std::vector<double> tms, tb;
+    for (auto &r : c->prof_recs) {
+        float e = 0;
+        TCG_CUDA(cudaEventElapsedTime(&e, r.a, r.b));
+        size_t i = 0;
+        for (; i < names.size(); i++)
+            if (names[i] == r.tag) break;
+        if (i == names.size()) { names.push_back(r.tag); cnt.push_back(0); tms.push_back(0); tb.push_back(0); }
+        cnt[i]++;
+        tms[i] += e;
+        tb[i] += r.bytes;
+    }
+    const int n = (int)std::min<size_t>(names.size(), (size_t)cap);
+    for (int i = 0; i < n; i++) {
+        if (tags) { memset(tags + 16 * i, 0, 16); strncpy(tags + 16 * i, names[i].c_str(), 15); }
+        if (count) count[i] = cnt[i];
+        if (ms) ms[i] = tms[i];
+        if (bytes) bytes[i] = tb[i];
+    }
+    *ntags = n;
     return TCG_OK;
 }

@@ -116,4 +116,8 @@ struct tcg_ctx {
     tcg::DBuf Rpsi, Rgpsi, acc2, acc3, qsum, tmp, tmp2, aux, items, meta;
     size_t tmp_budget = 0;                  // bytes per chunk of pass temporaries (0: default 1 GiB)
     int64_t launches = 0;
+    // optional per-kernel timing with CUDA events on the context stream
+    bool prof = false;
+    struct ProfRec { const void *fn; const char *tag; cudaEvent_t a, b; double bytes; };
+    std::vector<ProfRec> prof_recs;
 };

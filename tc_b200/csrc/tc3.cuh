@@ -412,16 +412,25 @@ static size_t max_items_for(const tcg_ctx *c, int nslots, size_t vbytes)
     return std::min<size_t>(65535, std::max<size_t>(1, budget / per));   // grid.y limit
 }
 
+// Algorithmic bytes per pass launch: a 3D FFT of N points moves 2 N s bytes
+// (one read + one write of the grid); each of the two passes of a
+// transform is credited half of it, N s per grid.
 template <typename T, class Op>
 static int run_chunk(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf = true, bool do_xyi = true)
 {
     using V = typename C2<T>::t;
     const GridDesc &g = c->gd;
     const int ntiles = (g.n0 * g.n1 + ZTC - 1) / ZTC;
-    if (do_xyf) TRY(launch(c, k_xyf<T, Op>, dim3(g.n2, items), dim3(256), smem_xy<V>(g), op));
-    TRY(launch(c, k_z<T, Op>, dim3(ntiles, items), dim3(256), smem_z<V>(g, Op::NF), op));
-    if (do_xyi)
-        TRY(launch(c, k_xyi<T, Op>, dim3(g.n2, nt), dim3(256), sizeof(V) * (3 * MAXN + (Op::GS + 2) * (size_t)g.n0 * g.n1), op));
+    const double gb = (double)g.N * sizeof(V);
+    if (do_xyf) TRY(launch_tagged(c, "xyf", (double)items * Op::NF * gb, k_xyf<T, Op>, dim3(g.n2, items), dim3(256), smem_xy<V>(g), op));
+    TRY(launch_tagged(c, "z", (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb, k_z<T, Op>, dim3(ntiles, items), dim3(256),
+                      smem_z<V>(g, Op::NF), op));
+    if (do_xyi) {
+        int nref = 0;
+        if (Op::REFWD) nref = Op::NB - 1;
+        TRY(launch_tagged(c, "xyi", (double)items * (Op::NB + nref) * gb, k_xyi<T, Op>, dim3(g.n2, nt), dim3(256),
+                          sizeof(V) * (3 * MAXN + (Op::GS + 2) * (size_t)g.n0 * g.n1), op));
+    }
     return TCG_OK;
 }
 

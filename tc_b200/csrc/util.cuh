@@ -41,7 +41,8 @@ template <typename V> inline size_t smem_z(const GridDesc &g, int nf) { return s
 inline std::mutex g_attr_mu;
 inline std::unordered_set<const void *> g_attr_set;
 template <typename K, typename... Args>
-inline int launch(tcg_ctx *c, K kernel, dim3 grid, dim3 block, size_t smem, Args... args)
+inline int launch_tagged(tcg_ctx *c, const char *tag, double alg_bytes, K kernel, dim3 grid, dim3 block, size_t smem,
+                         Args... args)
 {
     if (grid.x == 0 || grid.y == 0 || grid.z == 0) return TCG_OK;
     if (smem > 48 * 1024) {
@@ -52,10 +53,26 @@ inline int launch(tcg_ctx *c, K kernel, dim3 grid, dim3 block, size_t smem, Args
         }
     }
     if (smem > 227 * 1024) return fail(TCG_ERR_UNSUPPORTED, "kernel shared memory exceeds 227 KB");
+    tcg_ctx::ProfRec rec{(const void *)kernel, tag, nullptr, nullptr, alg_bytes};
+    if (c->prof) {
+        TCG_CUDA(cudaEventCreate(&rec.a));
+        TCG_CUDA(cudaEventCreate(&rec.b));
+        TCG_CUDA(cudaEventRecord(rec.a, c->stream));
+    }
     kernel<<<grid, block, smem, c->stream>>>(args...);
     c->launches++;
     TCG_CUDA(cudaGetLastError());
+    if (c->prof) {
+        TCG_CUDA(cudaEventRecord(rec.b, c->stream));
+        c->prof_recs.push_back(rec);
+    }
     return TCG_OK;
+}
+
+template <typename K, typename... Args>
+inline int launch(tcg_ctx *c, K kernel, dim3 grid, dim3 block, size_t smem, Args... args)
+{
+    return launch_tagged(c, "misc", 0.0, kernel, grid, block, smem, args...);
 }
 
 #define TRY(x)                     \
