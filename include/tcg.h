@@ -178,7 +178,7 @@ int tcg_sum_of_vaux(const tcg_system_desc *sys, double *alpha_out, double *sum_v
 int tcg_density(tcg_ctx *ctx, const tcg_state_desc *st, double *density_out);
 
 /* Tuning knob: bytes of pass temporaries one chunk of (target x source)
- * pairs may use (0 = default, 1 GiB).  Smaller chunks keep the temporaries
+ * pairs may use (0 = default, 8 GiB).  Smaller chunks keep the temporaries
  * resident in L2; larger ones launch fewer kernels.  No reference
  * counterpart (TC++ has no chunked pair pipeline). */
 int tcg_set_tuning(tcg_ctx *ctx, int64_t tmp_budget_bytes);
@@ -188,9 +188,9 @@ int tcg_set_tuning(tcg_ctx *ctx, int64_t tmp_budget_bytes);
  * reference counterpart (TC++ times whole phases at 1 s resolution,
  * my_clock.cpp:19-33). */
 int tcg_profile(tcg_ctx *ctx, int enable);
-/* Aggregate of the recorded launches per pass tag ("xyf", "z", "xyi",
- * "misc"): count, device milliseconds and algorithmic bytes (N s per grid
- * and pass; a 3D FFT = 2 N s).  tags: cap x 16 chars. */
+/* Aggregate of the recorded launches per "term:pass" tag (pass = xyf, z,
+ * xyi; "misc" for the rest): count, device milliseconds and algorithmic
+ * bytes (N s per grid and pass; a 3D FFT = 2 N s).  tags: cap x 32 chars. */
 int tcg_profile_read(tcg_ctx *ctx, int cap, char *tags, int64_t *count, double *ms, double *bytes, int *ntags);
 
 /* Device stream the context queues work on (cudaStream_t, as void*). */

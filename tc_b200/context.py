@@ -90,8 +90,8 @@ class Context:
 
     def profile_read(self):
         """{tag: (launches, device ms, algorithmic bytes)} of recorded launches."""
-        cap = 16
-        tags = C.create_string_buffer(16 * cap)
+        cap = 64
+        tags = C.create_string_buffer(32 * cap)
         cnt = (C.c_int64 * cap)()
         ms = (C.c_double * cap)()
         by = (C.c_double * cap)()
@@ -99,7 +99,7 @@ class Context:
         check(lib().tcg_profile_read(self.handle, cap, tags, cnt, ms, by, C.byref(n)))
         out = {}
         for i in range(n.value):
-            t = tags.raw[16 * i:16 * i + 16].split(b"\0")[0].decode()
+            t = tags.raw[32 * i:32 * i + 32].split(b"\0")[0].decode()
             out[t] = (int(cnt[i]), float(ms[i]), float(by[i]))
         return out
 

@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <mutex>
 #include <unordered_set>
 #include "ctx.cuh"
@@ -180,6 +181,12 @@ extern "C" int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg
         tcg_ctx_destroy(c);
         return fail(TCG_ERR_CUDA, "upload failed");
     }
+    if (h.n[0] == h.n[1] && h.n[1] == h.n[2]) {
+        const int fastn[] = {12, 16, 24, 32, 36, 40, 48};
+        for (int f : fastn)
+            if (h.n[0] == f) c->fast_n = f;
+    }
+    if (getenv("TCG_GENERIC_PASSES")) c->force_generic = true;
     *out = c;
     return TCG_OK;
 }
@@ -574,7 +581,7 @@ extern "C" int tcg_profile(tcg_ctx *c, int enable)
 // Aggregate the recorded launches per tag: for tag i writes count, total
 // device milliseconds and algorithmic bytes.  Returns the number of tags via
 // *ntags (<= cap).  Tags: "xyf", "z", "xyi", "misc".
-extern "C" int tcg_profile_read(tcg_ctx *c, int cap, char *tags /* cap x 16 */, int64_t *count, double *ms,
+extern "C" int tcg_profile_read(tcg_ctx *c, int cap, char *tags /* cap x 32 */, int64_t *count, double *ms,
                                 double *bytes, int *ntags)
 {
     if (!c || !ntags) return fail(TCG_ERR_ARG, "null argument");
@@ -595,7 +602,7 @@ extern "C" int tcg_profile_read(tcg_ctx *c, int cap, char *tags /* cap x 16 */, 
     }
     const int n = (int)std::min<size_t>(names.size(), (size_t)cap);
     for (int i = 0; i < n; i++) {
-        if (tags) { memset(tags + 16 * i, 0, 16); strncpy(tags + 16 * i, names[i].c_str(), 15); }
+        if (tags) { memset(tags + 32 * i, 0, 32); strncpy(tags + 32 * i, names[i].c_str(), 31); }
         if (count) count[i] = cnt[i];
         if (ms) ms[i] = tms[i];
         if (bytes) bytes[i] = tb[i];

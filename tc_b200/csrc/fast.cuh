@@ -1,0 +1,380 @@
+// fast.cuh -- compile-time-size pass kernels for cubic grids N^3.
+//
+// Each 1D transform of length N is held by ONE thread in registers and run
+// as a fully unrolled mixed-radix Stockham (all indices compile-time; no
+// integer division, no barrier inside a line).  Shared memory only
+// transposes planes between the x and y sweeps:
+//   XY pass: P planes per CTA, thread (plane, line); global -> smem
+//            (coalesced) -> row FFT (registers) -> smem -> column FFT
+//            (registers) -> global straight from registers (coalesced: the
+//            threads of a plane hold consecutive columns x).
+//   Z pass : one thread per (x, y) pencil, loaded from / stored to global
+//            straight from registers (consecutive threads = consecutive x);
+//            the NF transformed inputs are staged in shared memory for the
+//            G-space combination, each output is inverse-transformed in
+//            registers and stored.
+// Rows of a shared plane are padded to N+1 elements (odd stride for even N)
+// so that the row sweeps are free of bank conflicts.
+#pragma once
+#include "fft.cuh"
+
+namespace tcg {
+namespace fast {
+
+// ------------------------------------------------------ radix schedule --
+__host__ __device__ constexpr int radix_at(int n, int s)
+{
+    // greedy: 8s, 4s, 2s, then odd primes; s-th radix
+    int m = n, k = 0;
+    while (m % 8 == 0) { if (k == s) return 8; m /= 8; k++; }
+    while (m % 4 == 0) { if (k == s) return 4; m /= 4; k++; }
+    while (m % 2 == 0) { if (k == s) return 2; m /= 2; k++; }
+    for (int q = 3; m > 1; q += 2)
+        while (m % q == 0) { if (k == s) return q; m /= q; k++; }
+    return 1;
+}
+__host__ __device__ constexpr int nstages(int n)
+{
+    int s = 0;
+    while (radix_at(n, s) > 1) s++;
+    return s;
+}
+__host__ __device__ constexpr int ns_at(int n, int s)
+{
+    int p = 1;
+    for (int i = 0; i < s; i++) p *= radix_at(n, i);
+    return p;
+}
+
+template <typename V, int R, int DIR> __device__ __forceinline__ void dftR(V *v)
+{
+    if constexpr (R == 2) dft2<V, DIR>(v);
+    else if constexpr (R == 3) dft3<V, DIR>(v);
+    else if constexpr (R == 4) dft4<V, DIR>(v);
+    else if constexpr (R == 5) dft5<V, DIR>(v);
+    else if constexpr (R == 8) dft8<V, DIR>(v);
+    else static_assert(R == 2, "unsupported radix in the fast path");
+}
+
+// one Stockham stage over a register array (Govindaraju et al. 2008 form)
+template <typename V, int N, int DIR, int R, int NS>
+__device__ __forceinline__ void rstage(const V (&a)[N], V (&b)[N], const V *__restrict__ tw)
+{
+    constexpr int M = N / R;
+#pragma unroll
+    for (int j = 0; j < M; j++) {
+        const int k = j % NS;
+        V v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = a[j + r * M];
+        if (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                const int ti = k * r * (N / (NS * R));
+                if (ti != 0) {
+                    V w = tw[ti];
+                    if (DIR > 0) w.y = -w.y;
+                    v[r] = cmul(v[r], w);
+                }
+            }
+        }
+        dftR<V, R, DIR>(v);
+        const int d0 = (j / NS) * NS * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) b[d0 + r * NS] = v[r];
+    }
+}
+
+template <typename V, int N, int DIR, int S, bool DONE = (S >= nstages(N))>
+struct Stages {
+    static __device__ __forceinline__ void run(V (&a)[N], V (&b)[N], const V *tw)
+    {
+        rstage<V, N, DIR, radix_at(N, S), ns_at(N, S)>(a, b, tw);
+        Stages<V, N, DIR, S + 1>::run(b, a, tw);
+    }
+};
+template <typename V, int N, int DIR, int S>
+struct Stages<V, N, DIR, S, true> {
+    static __device__ __forceinline__ void run(V (&)[N], V (&)[N], const V *) {}
+};
+
+// In-register 1D FFT of x (result in x).  tw: N twiddles exp(-2 pi i j/N).
+template <typename V, int N, int DIR>
+__device__ __forceinline__ void line_fft(V (&x)[N], const V *__restrict__ tw)
+{
+    V y[N];
+    Stages<V, N, DIR, 0>::run(x, y, tw);
+    if constexpr (nstages(N) % 2 == 1) {
+#pragma unroll
+        for (int i = 0; i < N; i++) x[i] = y[i];
+    }
+}
+
+// planes per CTA (XY passes); two plane sets must fit in 227 KB of smem
+template <int N, int VB> struct Cfg {
+    static constexpr int P0 = (N <= 16) ? 12 : (N <= 24 ? 8 : 4);
+    static constexpr int PAD = N + ((N % 2 == 0) ? 1 : 0);           // row stride in smem
+    static constexpr int P = (2 * P0 * N * PAD * VB > 200 * 1024) ? P0 / 2 : P0;
+    static constexpr int THREADS = P * N;
+};
+
+// asynchronous global -> shared copy of one complex element (8 or 16 B)
+template <typename V>
+__device__ __forceinline__ void cp_async_elem(V *dst_smem, const V *src_gmem)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    if constexpr (sizeof(V) == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src_gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src_gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <typename V>
+__device__ __forceinline__ void stage_tw(const GridDesc &g, V *tws, int n)
+{
+    const V *src = twsrc<V>(g);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tws[i] = src[i];   // cubic grid: axis 0 table
+}
+
+// ---------------------------------------------------------------- XYF ----
+template <typename T, int N, class Op>
+__global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 3) k_xyf_fast(Op op, int nplanes)
+{
+    using V = typename C2<T>::t;
+    constexpr int P = Cfg<N, sizeof(typename C2<T>::t)>::P, PAD = Cfg<N, sizeof(typename C2<T>::t)>::PAD;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    V *A = tw + 128;
+    stage_tw<V>(op.g, tw, N);
+    const int pl = threadIdx.x / N, ln = threadIdx.x % N;
+    const int pid0 = blockIdx.x * P;
+    for (int f = 0; f < Op::NF; f++) {
+        __syncthreads();
+        // P*N*N elements, N per thread, loads batched by 4
+#pragma unroll 4
+        for (int k = 0; k < N; k++) {
+            const int e = threadIdx.x + k * (P * N);
+            const int q = e / (N * N), r = e % (N * N);
+            const int pid = pid0 + q;
+            if (pid < nplanes) {
+                const int item = pid / N, z = pid % N, x = r % N, y = r / N;
+                A[q * N * PAD + y * PAD + x] = op.xyf_load(item, f, x, y, z, (size_t)z * N * N + r);
+            }
+        }
+        __syncthreads();
+        V v[N];
+        V *row = A + pl * N * PAD + ln * PAD;
+#pragma unroll
+        for (int i = 0; i < N; i++) v[i] = row[i];
+        line_fft<V, N, -1>(v, tw);
+#pragma unroll
+        for (int i = 0; i < N; i++) row[i] = v[i];
+        __syncthreads();
+        const V *col = A + pl * N * PAD + ln;
+#pragma unroll
+        for (int i = 0; i < N; i++) v[i] = col[i * PAD];
+        line_fft<V, N, -1>(v, tw);
+        const int pid = pid0 + pl;
+        if (pid < nplanes) {
+            const int item = pid / N, z = pid % N;
+            V *dst = op.tmp_grid(item, f) + (size_t)z * N * N + ln;
+#pragma unroll
+            for (int i = 0; i < N; i++) dst[i * N] = v[i];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ Z ----
+// TC pencils per CTA, ZH threads per pencil: thread (h, c) transforms the
+// inputs f = h, h+ZH, ... and produces the outputs o = h, h+ZH, ...; the
+// forward-transformed inputs of all pencils are staged in smem [NF][N][TC].
+template <typename V> __host__ __device__ constexpr int zcols() { return 32; }
+constexpr int ZH = 4;
+
+template <typename T, int N, class Op>
+__global__ void __launch_bounds__(32 * ZH, 3) k_z_fast(Op op)
+{
+    using V = typename C2<T>::t;
+    constexpr int TC = zcols<V>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    V *S = tw + 128;                      // [NF][N][TC]
+    stage_tw<V>(op.g, tw, N);
+    __syncthreads();
+    const int item = blockIdx.y;
+    const int lane = threadIdx.x % TC, h = threadIdx.x / TC;
+    const int c = blockIdx.x * TC + lane;
+    const bool act = c < N * N;
+    const int x = c % N, y = c / N;
+    V v[N];
+    for (int f = h; f < Op::NF; f += ZH) {
+        if (act) {
+            const V *src = op.zin_grid(item, f) + c;
+#pragma unroll
+            for (int z = 0; z < N; z++) v[z] = src[(size_t)z * N * N];
+        } else {
+#pragma unroll
+            for (int z = 0; z < N; z++) v[z] = czero<V>();
+        }
+        line_fft<V, N, -1>(v, tw);
+        V *s = S + f * N * TC + lane;
+#pragma unroll
+        for (int z = 0; z < N; z++) s[z * TC] = v[z];
+    }
+    __syncthreads();
+    for (int o = h; o < Op::NB; o += ZH) {
+#pragma unroll
+        for (int z = 0; z < N; z++) {
+            V vin[Op::NF];
+#pragma unroll
+            for (int f = 0; f < Op::NF; f++) vin[f] = S[f * N * TC + z * TC + lane];
+            v[z] = act ? op.zmix(item, o, x, y, z, vin) : czero<V>();
+        }
+        if (Op::ZINV) line_fft<V, N, +1>(v, tw);
+        if (act) {
+            V *dst = op.out_grid(item, o) + c;
+#pragma unroll
+            for (int z = 0; z < N; z++) dst[(size_t)z * N * N] = v[z];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- XYI ----
+// smem: twiddles + GS planes-of-P (results of a group) + 1 work set
+template <typename T, int N, class Op>
+__global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2) k_xyi_fast(Op op, int nplanes)
+{
+    using V = typename C2<T>::t;
+    constexpr int P = Cfg<N, sizeof(typename C2<T>::t)>::P, PAD = Cfg<N, sizeof(typename C2<T>::t)>::PAD;
+    constexpr int PS = P * N * PAD;       // one set of P planes
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    V *W = tw + 128;                      // [GS + 1][P][N][PAD]
+    stage_tw<V>(op.g, tw, N);
+    const int pl = threadIdx.x / N, ln = threadIdx.x % N;
+    const int pid0 = blockIdx.x * P;
+    const int mypid = pid0 + pl;
+    const bool mine = mypid < nplanes;
+    const int tj = mine ? mypid / N : 0, z = mypid % N;
+    // all planes of the CTA must belong to targets with the same source count
+    const int ns = op.nsrc(pid0 / N);
+    // register accumulation only in the FP32 path (an FP64 column would
+    // double the register footprint of the line FFT)
+    constexpr bool RACC = Op::REGACC && sizeof(V) == 8;
+    V racc[RACC ? N : 1];
+#pragma unroll
+    for (int i = 0; i < (RACC ? N : 1); i++) racc[i] = czero<V>();
+    for (int si = 0; si < ns; si++) {
+        for (int b0 = 0; b0 < Op::NB; b0 += Op::GS) {
+            V *keepc = W + PS + pl * N * PAD + ln;      // set 1, this thread's column
+#pragma unroll
+            for (int q = 0; q < Op::GS; q++) {
+                V *A = W;
+                __syncthreads();
+                // plane copies global -> smem without passing through registers
+#pragma unroll 4
+                for (int k = 0; k < N; k++) {
+                    const int e = threadIdx.x + k * (P * N);
+                    const int qq = e / (N * N), r = e % (N * N);
+                    const int pid = pid0 + qq;
+                    if (pid < nplanes) {
+                        const int it = op.item_of(pid / N, si);
+                        cp_async_elem(A + qq * N * PAD + (r / N) * PAD + (r % N),
+                                      op.xyi_grid(it, b0 + q) + (size_t)(pid % N) * N * N + r);
+                    }
+                }
+                cp_async_wait_all();
+                __syncthreads();
+                V v[N];
+                V *row = A + pl * N * PAD + ln * PAD;
+#pragma unroll
+                for (int i = 0; i < N; i++) v[i] = row[i];
+                line_fft<V, N, +1>(v, tw);
+#pragma unroll
+                for (int i = 0; i < N; i++) row[i] = v[i];
+                __syncthreads();
+                const V *colp = A + pl * N * PAD + ln;
+#pragma unroll
+                for (int i = 0; i < N; i++) v[i] = colp[i * PAD];
+                line_fft<V, N, +1>(v, tw);
+                if (Op::GS > 1 && q < Op::GS - 1) {
+                    // keep this grid's column (thread-private) for the group accumulation
+#pragma unroll
+                    for (int i = 0; i < N; i++) keepc[i * PAD] = v[i];
+                } else if (mine) {
+                    const int item = op.item_of(tj, si);
+                    if (RACC && op.regacc_grid(b0)) {
+#pragma unroll
+                        for (int yy = 0; yy < N; yy++) {
+                            V vals[1] = {v[yy]};
+                            racc[yy] = cadd(racc[yy], op.xyi_term(tj, item, b0, (size_t)z * N * N + (size_t)yy * N + ln, vals));
+                        }
+                    } else {
+#pragma unroll
+                        for (int yy = 0; yy < N; yy++) {
+                            V vals[Op::GS];
+                            if constexpr (Op::GS > 1) { vals[0] = keepc[yy * PAD]; vals[Op::GS - 1] = v[yy]; }
+                            else vals[0] = v[yy];
+                            op.xyi_accum(tj, item, b0, (size_t)z * N * N + (size_t)yy * N + ln, vals);
+                        }
+                    }
+                }
+                if (Op::REFWD && Op::GS == 1) {
+                    // derived plane: column values -> forward column FFT -> smem -> forward rows -> global
+                    const bool want = op.refwd_want(b0);
+                    if (want) {
+                        const int item = op.item_of(tj, si);
+#pragma unroll
+                        for (int yy = 0; yy < N; yy++)
+                            v[yy] = mine ? op.refwd_load(tj, item, b0, (size_t)z * N * N + (size_t)yy * N + ln, v[yy])
+                                         : czero<V>();
+                        line_fft<V, N, -1>(v, tw);
+                        V *B = W + PS;          // work set
+                        V *cb = B + pl * N * PAD + ln;
+#pragma unroll
+                        for (int i = 0; i < N; i++) cb[i * PAD] = v[i];
+                        __syncthreads();
+                        V *rb = B + pl * N * PAD + ln * PAD;
+#pragma unroll
+                        for (int i = 0; i < N; i++) v[i] = rb[i];
+                        line_fft<V, N, -1>(v, tw);
+#pragma unroll
+                        for (int i = 0; i < N; i++) rb[i] = v[i];
+                        __syncthreads();
+#pragma unroll
+                        for (int k = 0; k < N; k++) {
+                            const int e = threadIdx.x + k * (P * N);
+                            const int qq = e / (N * N), r = e % (N * N);
+                            const int pid = pid0 + qq;
+                            if (pid < nplanes) {
+                                const int it = op.item_of(pid / N, si);
+                                op.refwd_grid(it, b0)[(size_t)(pid % N) * N * N + r] = B[qq * N * PAD + (r / N) * PAD + (r % N)];
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (RACC && mine) {
+#pragma unroll
+        for (int yy = 0; yy < N; yy++) op.xyi_flush(tj, (size_t)z * N * N + (size_t)yy * N + ln, racc[yy]);
+    }
+}
+
+template <typename V, int N> __host__ inline size_t smem_xy_fast(int sets)
+{
+    return sizeof(V) * (128 + (size_t)sets * Cfg<N, sizeof(V)>::P * N * Cfg<N, sizeof(V)>::PAD);
+}
+template <typename V, int N> __host__ inline size_t smem_z_fast(int nf)
+{
+    return sizeof(V) * (128 + (size_t)nf * N * zcols<V>());
+}
+
+} // namespace fast
+} // namespace tcg

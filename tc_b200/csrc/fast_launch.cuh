@@ -1,0 +1,30 @@
+// fast_launch.cuh -- launcher of the compile-time-size pass kernels (cubic
+// grids).  Algorithmic bytes per launch as in run_chunk: N s per grid and pass.
+#pragma once
+#include "terms.cuh"
+#include "fast.cuh"
+
+namespace tcg {
+
+template <typename T, int N, class Op>
+int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, bool do_xyi)
+{
+    using V = typename C2<T>::t;
+    using CF = fast::Cfg<N, sizeof(V)>;
+    const double gb = (double)N * N * N * sizeof(V);
+    const int np_f = items * N, np_i = nt * N;
+    if (do_xyf)
+        TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * Op::NF * gb, fast::k_xyf_fast<T, N, Op>,
+                          dim3((np_f + CF::P - 1) / CF::P), dim3(CF::THREADS), fast::smem_xy_fast<V, N>(1), op, np_f));
+    constexpr int TC = fast::zcols<V>();
+    TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb, fast::k_z_fast<T, N, Op>,
+                      dim3((N * N + TC - 1) / TC, items), dim3(TC * fast::ZH), fast::smem_z_fast<V, N>(Op::NF), op));
+    if (do_xyi) {
+        const int nref = Op::REFWD ? Op::NB - 1 : 0;
+        TRY(launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (Op::NB + nref) * gb, fast::k_xyi_fast<T, N, Op>,
+                          dim3((np_i + CF::P - 1) / CF::P), dim3(CF::THREADS), fast::smem_xy_fast<V, N>(2), op, np_i));
+    }
+    return TCG_OK;
+}
+
+} // namespace tcg

@@ -271,7 +271,7 @@ struct GatherItem {
     double2 fac;             // complex factor (includes 1/N)
 };
 
-__global__ void __launch_bounds__(256) k_gather_z(GridDesc g, const GatherItem *items)
+static __global__ void __launch_bounds__(256) k_gather_z(GridDesc g, const GatherItem *items)
 {
     using V = double2;
     extern __shared__ __align__(16) unsigned char smem_raw[];

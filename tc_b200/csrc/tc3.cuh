@@ -7,19 +7,19 @@
 namespace tcg {
 
 // ------------------------------------------------------------- utilities --
-__global__ void k_zero(double2 *p, size_t n)
+static __global__ void k_zero(double2 *p, size_t n)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = {0, 0};
 }
 
-__global__ void k_add(size_t n, const double2 *a, double2 *b)
+static __global__ void k_add(size_t n, const double2 *a, double2 *b)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         b[i] = cadd(b[i], a[i]);
 }
 
 // y += a x
-__global__ void k_axpy(size_t n, double a, const double2 *x, double2 *y)
+static __global__ void k_axpy(size_t n, double a, const double2 *x, double2 *y)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         y[i] = {y[i].x + a * x[i].x, y[i].y + a * x[i].y};
@@ -55,7 +55,7 @@ __global__ void k_dot3(int N, const double2 *a, const typename C2<T>::t *b, doub
 }
 
 // dnu_s[d](G) = sum_{s3} u(G; s, s3) G_d n_{s3}(G)   (tc3a1.cpp:53-70)
-__global__ void k_dnu_g(GridDesc g, RecipC rc, Jastrow J, int s, const double2 *nG, double2 *out)
+static __global__ void k_dnu_g(GridDesc g, RecipC rc, Jastrow J, int s, const double2 *nG, double2 *out)
 {
     const double zero[3] = {0, 0, 0};
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += gridDim.x * blockDim.x) {
@@ -74,7 +74,7 @@ __global__ void k_dnu_g(GridDesc g, RecipC rc, Jastrow J, int s, const double2 *
 }
 
 // V3a1(r) = sum_d dnu_d(r)^2 (complex square, tc3a1.cpp:78-84)
-__global__ void k_square_sum(int N, const double2 *dnu, double2 *V)
+static __global__ void k_square_sum(int N, const double2 *dnu, double2 *V)
 {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
         double2 s = {0, 0};
@@ -84,7 +84,7 @@ __global__ void k_square_sum(int N, const double2 *dnu, double2 *V)
 }
 
 // W_d = dnu_d(r) n(r)  (tc3b1.cpp:77-82)
-__global__ void k_mul_dens(int N, const double2 *dnu, const double2 *n, double2 *W)
+static __global__ void k_mul_dens(int N, const double2 *dnu, const double2 *n, double2 *W)
 {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x)
         for (int d = 0; d < 3; d++) W[(size_t)d * N + p] = cmul(dnu[(size_t)d * N + p], n[p]);
@@ -92,7 +92,7 @@ __global__ void k_mul_dens(int N, const double2 *dnu, const double2 *n, double2 
 
 // V(G) += sum_{s2} u(G; s1, s2) G . W[s2ref](G)    (tc3b1.cpp:86-101)
 // mode 1 (3b2, tc3a2a4b2b5.cpp:927-958): V(G) += fac * sum_d G_d u'(G) W_d(G)
-__global__ void k_gdot(GridDesc g, RecipC rc, Jastrow J, int s1, int nspin, const double2 *W0, const double2 *W1,
+static __global__ void k_gdot(GridDesc g, RecipC rc, Jastrow J, int s1, int nspin, const double2 *W0, const double2 *W1,
                        double2 *V, int mode, int sq)
 {
     const double zero[3] = {0, 0, 0};
@@ -119,7 +119,7 @@ __global__ void k_gdot(GridDesc g, RecipC rc, Jastrow J, int s1, int nspin, cons
 }
 
 // tG(G) = sum_js 4 pi n_js(G) A_{0,sj} u(G; 0, sj) [G != 0]   (tc3a3b3b4b6.cpp:96-107, 429-451)
-__global__ void k_div3b6_g(GridDesc g, RecipC rc, Jastrow J, double A00, double A01, int s, const double2 *nG,
+static __global__ void k_div3b6_g(GridDesc g, RecipC rc, Jastrow J, double A00, double A01, int s, const double2 *nG,
                            double2 *tG)
 {
     const double zero[3] = {0, 0, 0};
@@ -208,7 +208,7 @@ struct RotArgs {
     int tr;
 };
 // scalar: out[idx] += fac * phase * (tr ? conj(in) : in)
-__global__ void k_rot_scalar(GridDesc g, RotArgs ra, const double2 *in, double2 *out, double fac)
+static __global__ void k_rot_scalar(GridDesc g, RotArgs ra, const double2 *in, double2 *out, double fac)
 {
     const double TWOPI = 2.0 * 3.14159265358979323846;
     const int nr[3] = {g.n0, g.n1, g.n2};
@@ -234,7 +234,7 @@ __global__ void k_rot_scalar(GridDesc g, RotArgs ra, const double2 *in, double2 
     }
 }
 // vector (3 components, Cartesian U^+): out_d[idx] = +-phase * sum_e M[d][e] (tr ? conj(in_e) : in_e)
-__global__ void k_rot_vec(GridDesc g, RotArgs ra, const double2 *in, double2 *out)
+static __global__ void k_rot_vec(GridDesc g, RotArgs ra, const double2 *in, double2 *out)
 {
     const double TWOPI = 2.0 * 3.14159265358979323846;
     const int nr[3] = {g.n0, g.n1, g.n2};
@@ -270,7 +270,7 @@ __global__ void k_rot_vec(GridDesc g, RotArgs ra, const double2 *in, double2 *ou
 }
 
 // B = -conj(Q) for TC (tc3a2a4b2b5.cpp:662)
-__global__ void k_negconj(size_t n, const double2 *Q, double2 *B)
+static __global__ void k_negconj(size_t n, const double2 *Q, double2 *B)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         B[i] = {-Q[i].x, Q[i].y};
@@ -404,13 +404,33 @@ static int plan_chunks(tcg_ctx *c, DBuf &meta, int ntg, const std::vector<int> &
     return TCG_OK;
 }
 
+// targets per chunk: the XYI pass runs one CTA per (target, plane group)
+// and loops over the chunk's sources, so give it ~12 waves of CTAs
+static int min_targets(const tcg_ctx *c)
+{
+    const int n2 = c->h.n[2];
+    return std::max(1, (148 * 3 * 12 * 4 + n2 - 1) / n2);
+}
+
 // chunk budget: tmp slots bytes <= c->tmp_budget
 static size_t max_items_for(const tcg_ctx *c, int nslots, size_t vbytes)
 {
     const size_t per = (size_t)nslots * c->h.N * vbytes;
-    const size_t budget = c->tmp_budget ? c->tmp_budget : ((size_t)1 << 30);
+    const size_t budget = c->tmp_budget ? c->tmp_budget : ((size_t)8 << 30);
     return std::min<size_t>(65535, std::max<size_t>(1, budget / per));   // grid.y limit
 }
+
+// Algorithmic bytes per pass launch: a 3D FFT of N points moves 2 N s bytes
+// (one read + one write of the grid); each of the two passes of a
+// transform is credited half of it, N s per grid.
+// Fast-path launcher, defined in fast_launch.cuh and instantiated per grid
+// size in fast_inst.cu (one translation unit per N).
+template <typename T, int N, class Op>
+int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, bool do_xyi);
+
+// Algorithmic bytes per pass launch: a 3D FFT of N points moves 2 N s bytes
+// (one read + one write of the grid); each of the two passes of a
+// transform is credited half of it, N s per grid.
 
 // Algorithmic bytes per pass launch: a 3D FFT of N points moves 2 N s bytes
 // (one read + one write of the grid); each of the two passes of a
@@ -420,15 +440,27 @@ static int run_chunk(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf = 
 {
     using V = typename C2<T>::t;
     const GridDesc &g = c->gd;
+    if (c->fast_n && !c->force_generic) {
+        switch (c->fast_n) {
+        case 12: return run_chunk_fast<T, 12, Op>(c, op, items, nt, do_xyf, do_xyi);
+        case 16: return run_chunk_fast<T, 16, Op>(c, op, items, nt, do_xyf, do_xyi);
+        case 24: return run_chunk_fast<T, 24, Op>(c, op, items, nt, do_xyf, do_xyi);
+        case 32: return run_chunk_fast<T, 32, Op>(c, op, items, nt, do_xyf, do_xyi);
+        case 36: return run_chunk_fast<T, 36, Op>(c, op, items, nt, do_xyf, do_xyi);
+        case 40: return run_chunk_fast<T, 40, Op>(c, op, items, nt, do_xyf, do_xyi);
+        case 48: return run_chunk_fast<T, 48, Op>(c, op, items, nt, do_xyf, do_xyi);
+        default: break;
+        }
+    }
     const int ntiles = (g.n0 * g.n1 + ZTC - 1) / ZTC;
     const double gb = (double)g.N * sizeof(V);
-    if (do_xyf) TRY(launch_tagged(c, "xyf", (double)items * Op::NF * gb, k_xyf<T, Op>, dim3(g.n2, items), dim3(256), smem_xy<V>(g), op));
-    TRY(launch_tagged(c, "z", (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb, k_z<T, Op>, dim3(ntiles, items), dim3(256),
+    if (do_xyf) TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * Op::NF * gb, k_xyf<T, Op>, dim3(g.n2, items), dim3(256), smem_xy<V>(g), op));
+    TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb, k_z<T, Op>, dim3(ntiles, items), dim3(256),
                       smem_z<V>(g, Op::NF), op));
     if (do_xyi) {
         int nref = 0;
         if (Op::REFWD) nref = Op::NB - 1;
-        TRY(launch_tagged(c, "xyi", (double)items * (Op::NB + nref) * gb, k_xyi<T, Op>, dim3(g.n2, nt), dim3(256),
+        TRY(launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (Op::NB + nref) * gb, k_xyi<T, Op>, dim3(g.n2, nt), dim3(256),
                           sizeof(V) * (3 * MAXN + (Op::GS + 2) * (size_t)g.n0 * g.n1), op));
     }
     return TCG_OK;
@@ -507,7 +539,7 @@ struct DivItem {
 };
 
 // h += sum_b fill_b dc <chi_kb|psi> phi_kb   (hf2x.cpp:150-200, tc2x.cpp:409-511)
-__global__ void __launch_bounds__(256) k_div_2x(const DivItem *items)
+static __global__ void __launch_bounds__(256) k_div_2x(const DivItem *items)
 {
     const DivItem it = items[blockIdx.x];
     __shared__ double2 red[256];
@@ -628,7 +660,7 @@ static int run_hf2x(tcg_ctx *c, const Targets &Tg, double2 *acc)
         Sources S = sources_of(c, s);
         std::vector<ChunkPlan> plan;
         TRY(plan_chunks(c, c->meta, TR.n, TR.key, TR.cartk, (int)S.key.size(), S.key, S.cartq,
-                        max_items_for(c, 1, sizeof(V)), (640 + h.n[2] - 1) / h.n[2], plan));
+                        max_items_for(c, 1, sizeof(V)), min_targets(c), plan));
         for (const ChunkPlan &p : plan) {
             TRY(c->tmp.ensure((size_t)p.nt * p.ns * N * sizeof(V)));
             OpHF2X<T> op;
@@ -655,7 +687,7 @@ static int run_tc2x(tcg_ctx *c, const Targets &Tg, double2 *acc)
         Sources S = sources_of(c, s);
         std::vector<ChunkPlan> plan;
         TRY(plan_chunks(c, c->meta, TR.n, TR.key, TR.cartk, (int)S.key.size(), S.key, S.cartq,
-                        max_items_for(c, 4, sizeof(V)), (640 + h.n[2] - 1) / h.n[2], plan));
+                        max_items_for(c, 4, sizeof(V)), min_targets(c), plan));
         for (const ChunkPlan &p : plan) {
             TRY(c->tmp.ensure((size_t)p.nt * p.ns * 4 * N * sizeof(V)));
             TRY(gen_tables(c, p, TAB_TC2X, s));
@@ -697,7 +729,7 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
         // stages A + B
         std::vector<ChunkPlan> plan;
         TRY(plan_chunks(c, c->meta, TR.n, TR.key, TR.cartk, (int)S.key.size(), S.key, S.cartq,
-                        max_items_for(c, 13, sizeof(V)), (640 + h.n[2] - 1) / h.n[2], plan));
+                        max_items_for(c, 13, sizeof(V)), min_targets(c), plan));
         for (const ChunkPlan &p : plan) {
             const size_t items = (size_t)p.nt * p.ns;
             TRY(c->tmp.ensure(items * 7 * N * sizeof(V)));
@@ -758,7 +790,7 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
         }
         // stage C: 3b4 (:651-770)
         TRY(plan_chunks(c, c->meta, TR.n, TR.key, TR.cartk, (int)S.key.size(), S.key, S.cartq,
-                        max_items_for(c, 3, sizeof(V)), (640 + h.n[2] - 1) / h.n[2], plan));
+                        max_items_for(c, 3, sizeof(V)), min_targets(c), plan));
         for (const ChunkPlan &p : plan) {
             const size_t items = (size_t)p.nt * p.ns;
             TRY(c->tmp.ensure(items * 3 * N * sizeof(V)));
@@ -837,7 +869,7 @@ static int qp_stage(tcg_ctx *c)
         std::vector<ChunkPlan> plan;
         const int nsl = bitc ? 12 : 6;
         TRY(plan_chunks(c, c->meta, ntq, tkey, tcart, (int)S.key.size(), S.key, S.cartq,
-                        max_items_for(c, nsl, sizeof(V)), (640 + h.n[2] - 1) / h.n[2], plan));
+                        max_items_for(c, nsl, sizeof(V)), min_targets(c), plan));
         for (const ChunkPlan &p : plan) {
             const size_t items = (size_t)p.nt * p.ns;
             TRY(c->tmp.ensure(items * nsl * N * sizeof(V)));
@@ -1022,7 +1054,7 @@ static int run_tc3a2a4b2b5_band(tcg_ctx *c, const Targets &Tg, double2 *acc)
         Sources S = sources_of(c, s);
         std::vector<ChunkPlan> plan;
         TRY(plan_chunks(c, c->meta, TR.n, TR.key, TR.cartk, (int)S.key.size(), S.key, S.cartq,
-                        max_items_for(c, 4, sizeof(V)), (640 + h.n[2] - 1) / h.n[2], plan));
+                        max_items_for(c, 4, sizeof(V)), min_targets(c), plan));
         for (const ChunkPlan &p : plan) {
             TRY(c->tmp.ensure((size_t)p.nt * p.ns * 4 * N * sizeof(V)));
             TRY(gen_tables(c, p, TAB_U_SS, s));

@@ -62,6 +62,15 @@ __device__ __forceinline__ void xyz_of(const GridDesc &g, size_t p, int &x, int 
 }
 
 __device__ __forceinline__ void acc_add(double2 *a, double2 v, double f) { *a = {a->x + f * v.x, a->y + f * v.y}; }
+// fire-and-forget accumulation (red.global.add.f64): no load / store
+// round trip per update.  Every accumulator element is updated by one thread
+// only, so the updates of an element keep their program order and the sum
+// is deterministic.
+__device__ __forceinline__ void acc_red(double2 *a, double2 v, double f)
+{
+    atomicAdd(&a->x, f * v.x);
+    atomicAdd(&a->y, f * v.y);
+}
 
 // ---------------------------------------------------------------- sphere --
 template <typename T>
@@ -179,6 +188,13 @@ struct OpBase {
     __device__ V refwd_load(int, int, int, size_t, V v) const { return v; }
     __device__ V *refwd_grid(int, int) const { return nullptr; }
     __device__ V xyf_load(int, int, int, int, int, size_t) const { return czero<V>(); }
+    // register accumulation (fast XYI path, FP32): grids b with regacc_grid(b)
+    // contribute xyi_term(...) to a per-thread column sum flushed once per
+    // chunk with xyi_flush; the other grids go through xyi_accum.
+    static constexpr bool REGACC = false;
+    __device__ bool regacc_grid(int) const { return false; }
+    __device__ V xyi_term(int, int, int, size_t, const V *v) const { return v[0]; }
+    __device__ void xyi_flush(int, size_t, V) const {}
     __device__ int pair_id(int item) const { return m.tb[item / ns] * m.nSB + m.sb[item % ns]; }
     __device__ const double *kq_of(int item) const { return m.kq + 3 * pair_id(item); }
     __device__ const double *tab_of(int item) const { return m.tab + (size_t)pair_id(item) * g.N * m.ntab; }
@@ -188,6 +204,15 @@ struct OpBase {
 template <typename T>
 struct OpHF2X : OpBase<T> {
     using V = typename C2<T>::t;
+    static constexpr const char *NAME = "hf2x";
+    static constexpr bool REGACC = true;
+    __device__ bool regacc_grid(int) const { return true; }
+    __device__ V xyi_term(int, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        return cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p])), (decltype(v[0].x))fill[si]);
+    }
+    __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
     static constexpr int NF = 1, NB = 1;
     const V *Rpsi, *Rocc;     // chunk's first target / source
     double2 *acc;
@@ -195,7 +220,7 @@ struct OpHF2X : OpBase<T> {
     __device__ V xyf_load(int item, int, int, int, int, size_t p) const
     {
         const int tj = item / this->ns, si = item % this->ns;
-        return cmulc(Rocc[(size_t)si * this->g.N + p], Rpsi[(size_t)tj * this->g.N + p]);
+        return cmulc(__ldg(&Rocc[(size_t)si * this->g.N + p]), __ldg(&Rpsi[(size_t)tj * this->g.N + p]));
     }
     __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
     {
@@ -208,7 +233,7 @@ struct OpHF2X : OpBase<T> {
     __device__ void xyi_accum(int tj, int item, int, size_t p, const V *v) const
     {
         const int si = item % this->ns;
-        acc_add(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], Rocc[(size_t)si * this->g.N + p])), fill[si]);
+        acc_red(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p]))), fill[si]);
     }
 };
 
@@ -216,6 +241,17 @@ struct OpHF2X : OpBase<T> {
 template <typename T>
 struct OpTC2X : OpBase<T> {
     using V = typename C2<T>::t;
+    static constexpr const char *NAME = "tc2x";
+    static constexpr bool REGACC = true;
+    __device__ bool regacc_grid(int) const { return true; }
+    __device__ V xyi_term(int, int item, int b, size_t p, const V *v) const
+    {
+        const size_t N = this->g.N;
+        const int si = item % this->ns;
+        const V o = b == 0 ? __ldg(&Rocc[(size_t)si * N + p]) : __ldg(&Rgrad[((size_t)si * 3 + (b - 1)) * N + p]);
+        return cscale(cmul(v[0], o), (decltype(v[0].x))(b == 0 ? fill[si] : -fill[si]));
+    }
+    __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
     static constexpr int NF = 4, NB = 4;
     const V *Rpsi, *Rgpsi;        // [nt][N], [nt][3][N]
     const V *Rocc, *Rchi, *Rgrad; // [ns][N], [ns][N], [ns][3][N]
@@ -225,8 +261,8 @@ struct OpTC2X : OpBase<T> {
     {
         const size_t N = this->g.N;
         const int tj = item / this->ns, si = item % this->ns;
-        const V chi = Rchi[(size_t)si * N + p];
-        const V rhs = f == 0 ? Rpsi[(size_t)tj * N + p] : Rgpsi[((size_t)tj * 3 + (f - 1)) * N + p];
+        const V chi = __ldg(&Rchi[(size_t)si * N + p]);
+        const V rhs = f == 0 ? __ldg(&Rpsi[(size_t)tj * N + p]) : __ldg(&Rgpsi[((size_t)tj * 3 + (f - 1)) * N + p]);
         return cmulc(chi, rhs);     // tc2x.cpp:350, :374
     }
     __device__ V zmix(int item, int o, int x, int y, int z, const V *in) const
@@ -249,8 +285,8 @@ struct OpTC2X : OpBase<T> {
     {
         const size_t N = this->g.N;
         const int si = item % this->ns;
-        const V o = b == 0 ? Rocc[(size_t)si * N + p] : Rgrad[((size_t)si * 3 + (b - 1)) * N + p];
-        acc_add(acc + (size_t)tj * N + p, to64(cmul(v[0], o)), b == 0 ? fill[si] : -fill[si]);
+        const V o = b == 0 ? __ldg(&Rocc[(size_t)si * N + p]) : __ldg(&Rgrad[((size_t)si * 3 + (b - 1)) * N + p]);
+        acc_red(acc + (size_t)tj * N + p, to64(cmul(v[0], o)), b == 0 ? fill[si] : -fill[si]);
     }
 };
 
@@ -260,7 +296,7 @@ enum TabMode { TAB_TC2X = 0, TAB_U_SX = 1, TAB_U_SS = 2, TAB_U_QX = 3 };
 // TAB_U_SX : [u(G; 0, s), u(G; 1, s)]                        (tc3a3b3b4b6.cpp:208-217)
 // TAB_U_SS : [u(G; s, s)]                                    (tc3a3b3b4b6.cpp:679-686)
 // TAB_U_QX : [u(G; s, 0), u(G; s, 1)]                        (tc3a2a4b2b5.cpp:244-253)
-__global__ void k_tables(GridDesc g, RecipC rc, Jastrow J, int mode, int s, int npair, const double *kq, double *tab)
+static __global__ void k_tables(GridDesc g, RecipC rc, Jastrow J, int mode, int s, int npair, const double *kq, double *tab)
 {
     const int ntab = mode == TAB_U_SS ? 1 : 2;
     const size_t total = (size_t)npair * g.N;
@@ -284,6 +320,15 @@ __global__ void k_tables(GridDesc g, RecipC rc, Jastrow J, int mode, int s, int 
 template <typename T>
 struct OpTC3A : OpBase<T> {
     using V = typename C2<T>::t;
+    static constexpr const char *NAME = "3a3b6A";
+    static constexpr bool REGACC = false;   // register pressure outweighs the saved RMW here
+    __device__ bool regacc_grid(int b) const { return b == 0; }
+    __device__ V xyi_term(int, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        return cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p])), (decltype(v[0].x))(fill[si] * b3));
+    }
+    __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
     static constexpr int NF = 4, NB = 7;
     static constexpr bool REFWD = true;
     const V *Rpsi, *Rocc, *Rchi;  // [nt][N], [ns][N]
@@ -298,9 +343,9 @@ struct OpTC3A : OpBase<T> {
     {
         const size_t N = this->g.N;
         const int tj = item / this->ns, si = item % this->ns;
-        const V chi = Rchi[(size_t)si * N + p];
-        V rhs = Rpsi[(size_t)tj * N + p];
-        if (f > 0) rhs = cmul(dnu[(size_t)(f - 1) * N + p], rhs);   // dnu_phi (:236)
+        const V chi = __ldg(&Rchi[(size_t)si * N + p]);
+        V rhs = __ldg(&Rpsi[(size_t)tj * N + p]);
+        if (f > 0) rhs = cmul(__ldg(&dnu[(size_t)(f - 1) * N + p]), rhs);   // dnu_phi (:236)
         return cmulc(chi, rhs);
     }
     __device__ V zmix(int item, int o, int x, int y, int z, const V *in) const
@@ -324,19 +369,19 @@ struct OpTC3A : OpBase<T> {
     {
         const size_t N = this->g.N;
         const int si = item % this->ns;
-        const V phq = Rocc[(size_t)si * N + p];
+        const V phq = __ldg(&Rocc[(size_t)si * N + p]);
         if (b == 0) {
-            acc_add(acc + (size_t)tj * N + p, to64(cmul(v[0], phq)), fill[si] * b3);
+            acc_red(acc + (size_t)tj * N + p, to64(cmul(v[0], phq)), fill[si] * b3);
         } else {
             const int xs = (b - 1) / 3, d = (b - 1) % 3;
-            if (xs == s) acc_add(qsum + ((size_t)tj * 3 + d) * N + p, to64(cmul(v[0], phq)), 1.0);
+            if (xs == s) acc_red(qsum + ((size_t)tj * 3 + d) * N + p, to64(cmul(v[0], phq)), 1.0);
         }
     }
     __device__ bool refwd_want(int b) const { return b > 0; }
     __device__ V refwd_load(int, int, int b, size_t p, V v) const
     {
         const int xs = (b - 1) / 3;
-        return cmul(v, from64<V>(dens[(size_t)xs * this->g.N + p]));   // orbital * n_s2 (:332)
+        return cmul(v, from64<V>(__ldg(&dens[(size_t)xs * this->g.N + p])));   // orbital * n_s2 (:332)
     }
     __device__ V *refwd_grid(int item, int b) const { return tmp2 + ((size_t)item * 6 + (b - 1)) * this->g.N; }
 };
@@ -345,6 +390,15 @@ struct OpTC3A : OpBase<T> {
 template <typename T>
 struct OpTC3B : OpBase<T> {
     using V = typename C2<T>::t;
+    static constexpr const char *NAME = "3b6B";
+    static constexpr bool REGACC = true;
+    __device__ bool regacc_grid(int) const { return true; }
+    __device__ V xyi_term(int, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        return cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p])), (decltype(v[0].x))b6);
+    }
+    __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
     static constexpr int NF = 6, NB = 1;
     const V *Rocc;
     double2 *acc;
@@ -368,7 +422,7 @@ struct OpTC3B : OpBase<T> {
     __device__ void xyi_accum(int tj, int item, int, size_t p, const V *v) const
     {
         const int si = item % this->ns;
-        acc_add(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], Rocc[(size_t)si * this->g.N + p])), b6);
+        acc_red(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p]))), b6);
     }
 };
 
@@ -376,6 +430,15 @@ struct OpTC3B : OpBase<T> {
 template <typename T>
 struct OpTC3C : OpBase<T> {
     using V = typename C2<T>::t;
+    static constexpr const char *NAME = "3b4C";
+    static constexpr bool REGACC = true;
+    __device__ bool regacc_grid(int) const { return true; }
+    __device__ V xyi_term(int, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        return cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p])), (decltype(v[0].x))(b4 * fill[si]));
+    }
+    __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
     static constexpr int NF = 3, NB = 1;
     const V *Rocc, *Rchi;
     const double2 *qsum;      // [nt][3][N]
@@ -386,7 +449,7 @@ struct OpTC3C : OpBase<T> {
     {
         const size_t N = this->g.N;
         const int tj = item / this->ns, si = item % this->ns;
-        return cmulc(Rchi[(size_t)si * N + p], from64<V>(qsum[((size_t)tj * 3 + f) * N + p]));
+        return cmulc(__ldg(&Rchi[(size_t)si * N + p]), from64<V>(__ldg(&qsum[((size_t)tj * 3 + f) * N + p])));
     }
     __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
     {
@@ -402,7 +465,7 @@ struct OpTC3C : OpBase<T> {
     __device__ void xyi_accum(int tj, int item, int, size_t p, const V *v) const
     {
         const int si = item % this->ns;
-        acc_add(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], Rocc[(size_t)si * this->g.N + p])), b4 * fill[si]);
+        acc_red(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p]))), b4 * fill[si]);
     }
 };
 
@@ -411,6 +474,7 @@ struct OpTC3C : OpBase<T> {
 template <typename T, bool BITC>
 struct OpQP : OpBase<T> {
     using V = typename C2<T>::t;
+    static constexpr const char *NAME = "qp";
     static constexpr int NF = BITC ? 2 : 1, NB = BITC ? 12 : 6, GS = BITC ? 2 : 1;
     const V *Rq2, *Rq2c;          // targets phi_q2(r), chi_q2(r)  [nt][N]
     const V *Rocc, *Rchi;         // sources phi_q1, chi_q1        [ns][N]
@@ -421,8 +485,8 @@ struct OpQP : OpBase<T> {
     {
         const size_t N = this->g.N;
         const int tj = item / this->ns, si = item % this->ns;
-        if (f == 0) return cmulc(Rchi[(size_t)si * N + p], Rq2[(size_t)tj * N + p]);   // (:359)
-        return cmulc(Rocc[(size_t)si * N + p], Rq2c[(size_t)tj * N + p]);              // (:365)
+        if (f == 0) return cmulc(__ldg(&Rchi[(size_t)si * N + p]), __ldg(&Rq2[(size_t)tj * N + p]));   // (:359)
+        return cmulc(__ldg(&Rocc[(size_t)si * N + p]), __ldg(&Rq2c[(size_t)tj * N + p]));              // (:365)
     }
     __device__ V zmix(int item, int o, int x, int y, int z, const V *in) const
     {
@@ -449,15 +513,15 @@ struct OpQP : OpBase<T> {
         const double2 o1 = to64(v[0]);
         if (BITC) {
             const double2 o2 = to64(v[1]);
-            acc_add(A + (size_t)xr * N + p, cmulc(o2, o1), -f1);                  // -f1 orbital conj(orbital2)
+            acc_red(A + (size_t)xr * N + p, cmulc(o2, o1), -f1);                  // -f1 orbital conj(orbital2)
             if (xs == sq) {
-                acc_add(A + (size_t)(nspin + d) * N + p, to64(cmul(v[0], Rocc[(size_t)si * N + p])), f1);
-                const double2 cc = to64(cmul(cconj(v[1]), cconj(Rchi[(size_t)si * N + p])));
-                acc_add(A + (size_t)(nspin + 3 + d) * N + p, cc, -f1);               // (:428-430)
+                acc_red(A + (size_t)(nspin + d) * N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * N + p]))), f1);
+                const double2 cc = to64(cmul(cconj(v[1]), cconj(__ldg(&Rchi[(size_t)si * N + p]))));
+                acc_red(A + (size_t)(nspin + 3 + d) * N + p, cc, -f1);               // (:428-430)
             }
         } else {
-            acc_add(A + (size_t)xr * N + p, double2{o1.x * o1.x + o1.y * o1.y, 0.0}, -f1);   // (:404-406)
-            if (xs == sq) acc_add(A + (size_t)(nspin + d) * N + p, to64(cmul(v[0], Rocc[(size_t)si * N + p])), f1);
+            acc_red(A + (size_t)xr * N + p, double2{o1.x * o1.x + o1.y * o1.y, 0.0}, -f1);   // (:404-406)
+            if (xs == sq) acc_red(A + (size_t)(nspin + d) * N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * N + p]))), f1);
         }
     }
 };
@@ -466,6 +530,7 @@ struct OpQP : OpBase<T> {
 template <typename T>
 struct OpPairFwd : OpBase<T> {
     using V = typename C2<T>::t;
+    static constexpr const char *NAME = "pairfwd";
     static constexpr int NF = 2, NB = 2;
     static constexpr bool ZINV = false;
     const V *A0, *B0, *A1, *B1;   // item i: conj(A0_i) B0_i, conj(A1_i) B1_i, pointers per item via strides
@@ -487,6 +552,17 @@ struct OpPairFwd : OpBase<T> {
 template <typename T>
 struct OpBand : OpBase<T> {
     using V = typename C2<T>::t;
+    static constexpr const char *NAME = "band";
+    static constexpr bool REGACC = true;
+    __device__ bool regacc_grid(int) const { return true; }
+    __device__ V xyi_term(int, int item, int b, size_t p, const V *v) const
+    {
+        const size_t N = this->g.N;
+        const int si = item % this->ns;
+        if (b < 3) return cmul(__ldg(&Qt[((size_t)si * 3 + b) * N + p]), v[0]);
+        return cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * N + p])), (decltype(v[0].x))(fb5 * fill[si]));
+    }
+    __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
     static constexpr int NF = 4, NB = 4;
     const V *Rpsi;                // [nt][N]
     const V *Rocc, *Rchi;         // phi_q2sym, chi_q2sym [ns][N]
@@ -498,9 +574,9 @@ struct OpBand : OpBase<T> {
     {
         const size_t N = this->g.N;
         const int tj = item / this->ns, si = item % this->ns;
-        const V phj = Rpsi[(size_t)tj * N + p];
-        if (f == 0) return cmulc(Rchi[(size_t)si * N + p], phj);   // (:865)
-        return cmul(Bt[((size_t)si * 3 + (f - 1)) * N + p], phj);   // (:885)
+        const V phj = __ldg(&Rpsi[(size_t)tj * N + p]);
+        if (f == 0) return cmulc(__ldg(&Rchi[(size_t)si * N + p]), phj);   // (:865)
+        return cmul(__ldg(&Bt[((size_t)si * 3 + (f - 1)) * N + p]), phj);   // (:885)
     }
     __device__ V zmix(int item, int o, int x, int y, int z, const V *in) const
     {
@@ -522,8 +598,8 @@ struct OpBand : OpBase<T> {
         const size_t N = this->g.N;
         const int si = item % this->ns;
         double2 *a = acc + (size_t)tj * N + p;
-        if (b < 3) acc_add(a, to64(cmul(Qt[((size_t)si * 3 + b) * N + p], v[0])), 1.0);    // (:875)
-        else acc_add(a, to64(cmul(v[0], Rocc[(size_t)si * N + p])), fb5 * fill[si]);      // (:894)
+        if (b < 3) acc_red(a, to64(cmul(__ldg(&Qt[((size_t)si * 3 + b) * N + p]), v[0])), 1.0);    // (:875)
+        else acc_red(a, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * N + p]))), fb5 * fill[si]);      // (:894)
     }
 };
 

@@ -1,6 +1,8 @@
 // util.cuh -- error helpers, kernel launch wrapper, upload helper.
 #pragma once
 #include <mutex>
+#include <string>
+#include <vector>
 #include <unordered_set>
 #include "ctx.cuh"
 #include "passes.cuh"
@@ -40,6 +42,19 @@ template <typename V> inline size_t smem_z(const GridDesc &g, int nf) { return s
 // Launch with the dynamic-smem attribute set once per kernel.
 inline std::mutex g_attr_mu;
 inline std::unordered_set<const void *> g_attr_set;
+// interned "op:pass" profiling tags
+inline const char *tagname(const char *op, const char *pass)
+{
+    static std::mutex mu;
+    static std::vector<std::string *> pool;
+    std::lock_guard<std::mutex> lk(mu);
+    std::string s = std::string(op) + ":" + pass;
+    for (auto *p : pool)
+        if (*p == s) return p->c_str();
+    pool.push_back(new std::string(s));
+    return pool.back()->c_str();
+}
+
 template <typename K, typename... Args>
 inline int launch_tagged(tcg_ctx *c, const char *tag, double alg_bytes, K kernel, dim3 grid, dim3 block, size_t smem,
                          Args... args)
@@ -49,6 +64,7 @@ inline int launch_tagged(tcg_ctx *c, const char *tag, double alg_bytes, K kernel
         std::lock_guard<std::mutex> lk(g_attr_mu);
         if (!g_attr_set.count((const void *)kernel)) {
             TCG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+            TCG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
             g_attr_set.insert((const void *)kernel);
         }
     }

@@ -145,3 +145,55 @@ def test_errors():
         with pytest.raises(TCError) as e:
             ctx.apply(abi.TERMS_TC, psi=bad)
         assert e.value.code == abi.TCG_ERR_NUMERIC
+
+
+@pytest.mark.parametrize("nr", [(24, 24, 24), (36, 36, 36)])
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_fast_path_sizes(nr, prec, tol):
+    """compile-time-size pass kernels at production grid sizes"""
+    s = system("BITC", nr=nr, nk=2, ecut=2.0, nbands=2, nocc=1)
+    r2, r3 = oracle_terms(s, abi.TERMS_TC)
+    with Context(s, prec) as ctx:
+        ctx.set_state()
+        g2, g3 = ctx.apply(abi.TERMS_TC)
+    assert rel(g2, r2) < tol
+    assert rel(g3, r3) < tol
+
+
+@pytest.mark.parametrize("method", ["HF", "BITC"])
+def test_generic_path_noncubic(method):
+    """non-cubic grid -> generic (runtime-size) pass kernels"""
+    s = system(method, nr=(12, 15, 10), nk=1, ecut=1.2, nbands=2, nocc=1)
+    mask = abi.TERMS_HF if method == "HF" else abi.TERMS_TC
+    r2, r3 = oracle_terms(s, mask)
+    with Context(s, "fp64") as ctx:
+        ctx.set_state()
+        g2, g3 = ctx.apply(mask)
+    assert rel(g2, r2) < FP64_TOL
+    if method != "HF":
+        assert rel(g3, r3) < FP64_TOL
+
+
+def test_generic_path_forced(monkeypatch):
+    """cubic grid with the generic kernels forced must agree too"""
+    monkeypatch.setenv("TCG_GENERIC_PASSES", "1")
+    s = system("TC")
+    r2, r3 = oracle_terms(s, abi.TERMS_TC)
+    with Context(s, "fp64") as ctx:
+        ctx.set_state()
+        g2, g3 = ctx.apply(abi.TERMS_TC)
+    assert rel(g2, r2) < FP64_TOL
+    assert rel(g3, r3) < FP64_TOL
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_bitwise_deterministic(prec):
+    """fixed-order accumulation: two applies give identical bits"""
+    s = system("BITC")
+    with Context(s, prec) as ctx:
+        ctx.set_state()
+        a2, a3 = ctx.apply(abi.TERMS_TC)
+        ctx.refresh_state()
+        b2, b3 = ctx.apply(abi.TERMS_TC)
+    assert np.array_equal(a2.view(np.uint64), b2.view(np.uint64))
+    assert np.array_equal(a3.view(np.uint64), b3.view(np.uint64))
