@@ -190,56 +190,120 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 3)
 }
 
 // ------------------------------------------------------------------ Z ----
-// TC pencils per CTA, ZH threads per pencil: thread (h, c) transforms the
-// inputs f = h, h+ZH, ... and produces the outputs o = h, h+ZH, ...; the
-// forward-transformed inputs of all pencils are staged in smem [NF][N][TC].
+// Each z-line is split over a lane pair (s = lane & 1):
+//   forward : one radix-2 DIF step across the pair via shuffles,
+//             X[2k+s] = FFT_{N/2}( s ? (x[n] - x[n+N/2]) w^n : x[n] + x[n+N/2] )
+//   inverse : FFT_{N/2} of the lane's half (frequencies 2k+s), then the
+//             radix-2 DIT combine across the pair, y[n + s N/2] = E -+ w^-n O.
+// Each thread holds N/2 values, so twice as many warps stay resident as
+// with one thread per line.  Lanes keep the frequencies z = 2k+s for the
+// G-space combination.  A CTA of 128 threads = 32 pencils x 2 halves x 2
+// groups; group h handles inputs f = h, h+2, ... and outputs o = h, h+2, ...
 template <typename V> __host__ __device__ constexpr int zcols() { return 32; }
-constexpr int ZH = 4;
+constexpr int ZH = 2;
+
+template <typename V>
+__device__ __forceinline__ V shfl_xor1(V v)
+{
+    V r;
+    r.x = __shfl_xor_sync(0xffffffffu, v.x, 1);
+    r.y = __shfl_xor_sync(0xffffffffu, v.y, 1);
+    return r;
+}
+
+// forward split transform: in natural order x[s*M + i] -> out X[2k+s]
+template <typename V, int N>
+__device__ __forceinline__ void fwd_split(V (&v)[N / 2], int s, const V *tw, const V *twM)
+{
+    constexpr int M = N / 2;
+#pragma unroll
+    for (int i = 0; i < M; i++) {
+        const V o = shfl_xor1(v[i]);
+        if (s == 0) v[i] = cadd(v[i], o);
+        else {
+            V d = csub(o, v[i]);              // x[i] - x[i+M]
+            if (i != 0) d = cmul(d, tw[i]);
+            v[i] = d;
+        }
+    }
+    line_fft<V, M, -1>(v, twM);
+}
+
+// inverse split transform: in Y[2k+s] -> out natural y[s*M + n]
+template <typename V, int N>
+__device__ __forceinline__ void inv_split(V (&v)[N / 2], int s, const V *tw, const V *twM)
+{
+    constexpr int M = N / 2;
+    line_fft<V, M, +1>(v, twM);               // s=0: E[n], s=1: O[n]
+#pragma unroll
+    for (int i = 0; i < M; i++) {
+        const V o = shfl_xor1(v[i]);
+        // s=0: y[n] = E + w^-n O ; s=1: y[n+M] = E - w^-n O
+        V odd = s == 0 ? o : v[i];
+        const V even = s == 0 ? v[i] : o;
+        if (i != 0) { V w = tw[i]; w.y = -w.y; odd = cmul(odd, w); }
+        v[i] = s == 0 ? cadd(even, odd) : csub(even, odd);
+    }
+}
 
 template <typename T, int N, class Op>
-__global__ void __launch_bounds__(32 * ZH, 3) k_z_fast(Op op)
+__global__ void __launch_bounds__(128, Op::ZMINB) k_z_fast(Op op)
 {
     using V = typename C2<T>::t;
-    constexpr int TC = zcols<V>();
+    constexpr int TC = 32, M = N / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    V *tw = reinterpret_cast<V *>(smem_raw);
-    V *S = tw + 128;                      // [NF][N][TC]
+    V *tw = reinterpret_cast<V *>(smem_raw);   // [N]: exp(-2 pi i j/N)
+    V *twM = tw + 64;                          // [M]: exp(-2 pi i j/M)
+    V *S = tw + 128;                           // [NF][N][TC]
     stage_tw<V>(op.g, tw, N);
     __syncthreads();
+    for (int i = threadIdx.x; i < M; i += blockDim.x) twM[i] = tw[2 * i];
+    __syncthreads();
     const int item = blockIdx.y;
-    const int lane = threadIdx.x % TC, h = threadIdx.x / TC;
-    const int c = blockIdx.x * TC + lane;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int s = lane & 1;
+    const int cl = (w & 1) * 16 + (lane >> 1);   // pencil within the CTA
+    const int h = w >> 1;                         // group
+    const int c = blockIdx.x * TC + cl;
     const bool act = c < N * N;
     const int x = c % N, y = c / N;
-    V v[N];
+    V v[M];
     for (int f = h; f < Op::NF; f += ZH) {
         if (act) {
-            const V *src = op.zin_grid(item, f) + c;
+            const V *src = op.zin_grid(item, f) + c + (size_t)s * M * N * N;
 #pragma unroll
-            for (int z = 0; z < N; z++) v[z] = src[(size_t)z * N * N];
+            for (int i = 0; i < M; i++) v[i] = src[(size_t)i * N * N];
         } else {
 #pragma unroll
-            for (int z = 0; z < N; z++) v[z] = czero<V>();
+            for (int i = 0; i < M; i++) v[i] = czero<V>();
         }
-        line_fft<V, N, -1>(v, tw);
-        V *s = S + f * N * TC + lane;
+        fwd_split<V, N>(v, s, tw, twM);
+        V *st = S + f * N * TC + cl;
 #pragma unroll
-        for (int z = 0; z < N; z++) s[z * TC] = v[z];
+        for (int k = 0; k < M; k++) st[(2 * k + s) * TC] = v[k];
     }
     __syncthreads();
     for (int o = h; o < Op::NB; o += ZH) {
 #pragma unroll
-        for (int z = 0; z < N; z++) {
+        for (int k = 0; k < M; k++) {
+            const int z = 2 * k + s;
             V vin[Op::NF];
 #pragma unroll
-            for (int f = 0; f < Op::NF; f++) vin[f] = S[f * N * TC + z * TC + lane];
-            v[z] = act ? op.zmix(item, o, x, y, z, vin) : czero<V>();
+            for (int f = 0; f < Op::NF; f++) vin[f] = S[f * N * TC + z * TC + cl];
+            v[k] = act ? op.zmix(item, o, x, y, z, vin) : czero<V>();
         }
-        if (Op::ZINV) line_fft<V, N, +1>(v, tw);
-        if (act) {
+        if (Op::ZINV) {
+            inv_split<V, N>(v, s, tw, twM);
+            if (act) {
+                V *dst = op.out_grid(item, o) + c + (size_t)s * M * N * N;
+#pragma unroll
+                for (int i = 0; i < M; i++) dst[(size_t)i * N * N] = v[i];
+            }
+        } else if (act) {
+            // G-space output: frequencies 2k+s
             V *dst = op.out_grid(item, o) + c;
 #pragma unroll
-            for (int z = 0; z < N; z++) dst[(size_t)z * N * N] = v[z];
+            for (int k = 0; k < M; k++) dst[(size_t)(2 * k + s) * N * N] = v[k];
         }
     }
 }

@@ -168,6 +168,7 @@ struct OpBase {
     using V = typename C2<T>::t;
     static constexpr bool ZINV = true, REFWD = false;
     static constexpr int GS = 1;
+    static constexpr int ZMINB = 3;          // min resident CTAs of the fast Z pass (register cap)
     GridDesc g;
     V *tmp;
     int nsl;                // tmp slots per item
