@@ -171,6 +171,25 @@ int tcg_apply_device(tcg_ctx *ctx, uint32_t term_mask, const int32_t *nb_apply,
  * and k-point fields of sys (sum_Vaux / alpha_Vaux of sys are ignored). */
 int tcg_sum_of_vaux(const tcg_system_desc *sys, double *alpha_out, double *sum_vaux_out);
 
+/* Allocation-free variant of tcg_sum_of_vaux for callers that cannot
+ * allocate device memory -- e.g. code running inside a stream capture or
+ * under an external memory pool that forbids cudaMalloc / cudaFree.  No
+ * counterpart in the reference (TC++ computes these sums on the host).
+ * All arrays are DEVICE pointers: kirr_dev [nk_irr][3] and kall_dev
+ * [nk_all][3] fractional k-vectors (irreducible k, full SCF mesh), output
+ * sum_vaux_dev [nk_irr]; alpha_out is a host pointer (may be NULL).  The
+ * work is queued on `stream` (cudaStream_t as void*, NULL = default) and the
+ * call returns after it finished.  Scratch is a static device array of
+ * 16384 (k, q) pairs held by every GPU that loads the library; larger
+ * nk_irr * nk_all is rejected with TCG_ERR_ARG.  The first call on a device
+ * looks the array's device address up (cudaGetSymbolAddress) and should
+ * come before any stream capture.  Every call shares the one array: calls
+ * that overlap on the GPU (other threads or streams) race and must be
+ * serialised by the caller. */
+int tcg_sum_of_vaux_noalloc(const double recip[9], double omega, int32_t nk_irr, int32_t nk_all,
+                            const double *kirr_dev, const double *kall_dev, double *sum_vaux_dev,
+                            double *alpha_out, void *stream);
+
 /* n_s(r) of the given orbitals (BlochStates::set_density, first iteration,
  * bloch_states_scfloop_filling_density.cpp:256-360), computed on the device;
  * density_out is [2][N] complex.  Fails with TCG_ERR_NUMERIC if an orbital's

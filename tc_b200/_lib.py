@@ -43,6 +43,8 @@ def lib():
         L.tcg_profile_read.argtypes = [vp, C.c_int, C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double),
                                        C.POINTER(C.c_double), C.POINTER(C.c_int)]
         L.tcg_refresh_state.argtypes = [vp]
+        L.tcg_sum_of_vaux_noalloc.argtypes = [C.POINTER(C.c_double), C.c_double, C.c_int32, C.c_int32, vp, vp, vp,
+                                              C.POINTER(C.c_double), vp]
         _lib = L
     return _lib
 
@@ -54,4 +56,5 @@ def check(rc):
 
 EXPORTS = ["tcg_ctx_create", "tcg_ctx_destroy", "tcg_set_state", "tcg_apply", "tcg_apply_device",
            "tcg_sum_of_vaux", "tcg_density", "tcg_stream", "tcg_launch_count", "tcg_last_error",
-           "tcg_version", "tcg_set_tuning", "tcg_profile", "tcg_profile_read", "tcg_refresh_state"]
+           "tcg_version", "tcg_set_tuning", "tcg_profile", "tcg_profile_read", "tcg_refresh_state",
+           "tcg_sum_of_vaux_noalloc"]

@@ -147,5 +147,16 @@ def sum_of_vaux(system):
     return alpha.value, out
 
 
+def sum_of_vaux_noalloc(system, kirr_dev_ptr, kall_dev_ptr, out_dev_ptr, stream=None):
+    """Allocation-free divergence sums: device pointers in, device pointer
+    out (see tcg_sum_of_vaux_noalloc in include/tcg.h).  Returns alpha."""
+    rec = (C.c_double * 9)(*[float(x) for x in np.asarray(system.recip).ravel()])
+    alpha = C.c_double()
+    check(lib().tcg_sum_of_vaux_noalloc(rec, float(system.omega), int(system.nk_irr), int(system.nk_all),
+                                        C.c_void_p(kirr_dev_ptr), C.c_void_p(kall_dev_ptr), C.c_void_p(out_dev_ptr),
+                                        C.byref(alpha), C.c_void_p(stream) if stream else None))
+    return alpha.value
+
+
 def version():
     return lib().tcg_version().decode()

@@ -610,3 +610,96 @@ extern "C" int tcg_profile_read(tcg_ctx *c, int cap, char *tags /* cap x 32 */, 
     *ntags = n;
     return TCG_OK;
 }
+
+// ------------------------------------- allocation-free divergence sums --
+// Scratch of tcg_sum_of_vaux_noalloc: one partial shell sum and one flag
+// word per (irreducible k, mesh q) pair, plus an error word.  File-scope
+// device arrays: every GPU that loads the library holds them (about 192 KiB)
+// until the process exits; no call allocates.
+constexpr int TCG_NOALLOC_MAX_PAIRS = 16384;
+static __device__ __align__(256) double g_noalloc_partial[TCG_NOALLOC_MAX_PAIRS];
+static __device__ __align__(256) int g_noalloc_flags[TCG_NOALLOC_MAX_PAIRS];
+static __device__ __align__(256) int g_noalloc_err[1];
+
+struct NoallocScratch {
+    double *partial = nullptr;
+    int *flags = nullptr;
+    int *err = nullptr;
+};
+static std::mutex g_noalloc_mu;
+static NoallocScratch g_noalloc_dev[64];
+
+// Device addresses of the scratch arrays on the current device.  Host code
+// only holds a host-side stand-in for a __device__ array's name, so the
+// address is looked up once per device with that device current.
+static int noalloc_scratch(NoallocScratch &out)
+{
+    int dev = 0;
+    TCG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(TCG_ERR_UNSUPPORTED, "device index >= 64");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoallocScratch &s = g_noalloc_dev[dev];
+    if (!s.partial) {
+        NoallocScratch t;
+        TCG_CUDA(cudaGetSymbolAddress((void **)&t.partial, g_noalloc_partial));
+        TCG_CUDA(cudaGetSymbolAddress((void **)&t.flags, g_noalloc_flags));
+        TCG_CUDA(cudaGetSymbolAddress((void **)&t.err, g_noalloc_err));
+        s = t;
+    }
+    out = s;
+    return TCG_OK;
+}
+
+// sum over the mesh q of one irreducible k, in q order (as tcg_sum_of_vaux)
+static __global__ void k_sum_vaux_final(int nk, int nk_all, const double *partial, const int *flags, double alpha,
+                                        double *sum_out, int *err)
+{
+    const double FOURPI = 4.0 * 3.14159265358979323846;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nk) return;
+    double total = 0.0;
+    int match = 0, bad = 0;
+    for (int a = 0; a < nk_all; a++) {
+        const int f = flags[(size_t)k * nk_all + a];
+        match |= f & 1;
+        bad |= f & 2;
+        total += partial[(size_t)k * nk_all + a];
+    }
+    total *= FOURPI;
+    if (match) total -= FOURPI * alpha;
+    sum_out[k] = total;
+    if (bad) atomicOr(err, 1);
+}
+
+extern "C" int tcg_sum_of_vaux_noalloc(const double recip[9], double omega, int32_t nk_irr, int32_t nk_all,
+                                       const double *kirr_dev, const double *kall_dev, double *sum_vaux_dev,
+                                       double *alpha_out, void *stream)
+{
+    if (!recip || !kirr_dev || !kall_dev || !sum_vaux_dev) return fail(TCG_ERR_ARG, "null argument");
+    if (!(omega > 0)) return fail(TCG_ERR_ARG, "unit-cell volume must be positive");
+    if (nk_irr < 1 || nk_all < 1) return fail(TCG_ERR_ARG, "no k-points");
+    if ((int64_t)nk_irr * nk_all > TCG_NOALLOC_MAX_PAIRS)
+        return fail(TCG_ERR_ARG, "nk_irr * nk_all exceeds the 16384 (k, q) pairs of the static scratch");
+    NoallocScratch sc;
+    TRY(noalloc_scratch(sc));
+    cudaStream_t st = (cudaStream_t)stream;
+    const double PI = 3.14159265358979323846;
+    double alpha = cbrt(omega) / (2.0 * PI);
+    alpha = alpha * alpha;
+    RecipC rc;
+    memcpy(rc.R, recip, sizeof rc.R);
+    // every partial / flag used below is written by k_sum_vaux before it is
+    // read; only the error word has to start at zero
+    TCG_CUDA(cudaMemsetAsync(sc.err, 0, sizeof(int), st));
+    k_sum_vaux<<<nk_irr * nk_all, 256, 0, st>>>(nk_all, kirr_dev, kall_dev, rc, alpha, sc.partial, sc.flags, 400);
+    TCG_CUDA(cudaGetLastError());
+    k_sum_vaux_final<<<(nk_irr + 127) / 128, 128, 0, st>>>(nk_irr, nk_all, sc.partial, sc.flags, alpha, sum_vaux_dev,
+                                                           sc.err);
+    TCG_CUDA(cudaGetLastError());
+    int err = 0;
+    TCG_CUDA(cudaMemcpyAsync(&err, sc.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TCG_CUDA(cudaStreamSynchronize(st));
+    if (err) return fail(TCG_ERR_NUMERIC, "divergence shell sum did not converge");
+    if (alpha_out) *alpha_out = alpha;
+    return TCG_OK;
+}

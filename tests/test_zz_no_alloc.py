@@ -1,0 +1,50 @@
+"""The allocation-free divergence-sum entry point (tcg_sum_of_vaux_noalloc)
+against the regular one (tcg_sum_of_vaux), on two calls in a row.
+
+Callers that cannot allocate device memory (stream capture, external pools)
+pass device inputs / outputs and the library works in a static device
+array.  This file is collected last so a failure here does not hide the
+other GPU tests; it must also pass alone in a fresh process."""
+import numpy as np
+import pytest
+
+from tc_b200 import synth
+from tc_b200.context import sum_of_vaux, sum_of_vaux_noalloc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["C1", "small-tr"])
+def test_noalloc_matches_regular_twice(name):
+    import torch
+    s = synth.config("C1") if name == "C1" else synth.small("TC", tr=True)
+    alpha_ref, ref = sum_of_vaux(s)
+    kirr = np.ascontiguousarray(s.kvec[s.kall_off[:-1]])
+    dev = torch.device("cuda", 0)
+    kirr_t = torch.from_numpy(kirr).to(dev)
+    kall_t = torch.from_numpy(np.ascontiguousarray(s.kvec)).to(dev)
+    for _ in range(2):
+        out = torch.full((s.nk_irr,), float("nan"), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        alpha = sum_of_vaux_noalloc(s, kirr_t.data_ptr(), kall_t.data_ptr(), out.data_ptr())
+        got = out.cpu().numpy()
+        assert abs(alpha - alpha_ref) <= 1e-15 * abs(alpha_ref)
+        assert np.all(np.isfinite(got))
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_noalloc_rejects_oversize():
+    import torch
+    from tc_b200 import TCError
+    s = synth.config("C1")
+    dev = torch.device("cuda", 0)
+    k = torch.zeros((200, 3), dtype=torch.float64, device=dev)
+    out = torch.zeros(200, dtype=torch.float64, device=dev)
+
+    class Big:
+        recip = s.recip
+        omega = s.omega
+        nk_irr = 200
+        nk_all = 200
+    with pytest.raises(TCError):
+        sum_of_vaux_noalloc(Big, k.data_ptr(), k.data_ptr(), out.data_ptr())
