@@ -197,3 +197,18 @@ def test_bitwise_deterministic(prec):
         b2, b3 = ctx.apply(abi.TERMS_TC)
     assert np.array_equal(a2.view(np.uint64), b2.view(np.uint64))
     assert np.array_equal(a3.view(np.uint64), b3.view(np.uint64))
+
+
+@pytest.mark.parametrize("name", ["small_hf", "small_tc", "small_bitc", "small_bitc_tr"])
+def test_gpu_matches_golden_fixture(name):
+    """CUDA path (FP64) against the committed oracle fixtures"""
+    import os
+    from golden.make_golden import mask_of, system
+    s = system(name)
+    ref = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    with Context(s, "fp64") as ctx:
+        ctx.set_state()
+        g2, g3 = ctx.apply(mask_of(s))
+    for got, want in ((g2, ref["h2"]), (g3, ref["h3"])):
+        if np.abs(want).max() > 0:
+            assert rel(got, want) < FP64_TOL
