@@ -196,7 +196,7 @@ extern "C" int tcg_ctx_destroy(tcg_ctx *c)
     if (!c) return TCG_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     DBuf *bufs[] = {&c->tw64, &c->tw32, &c->recip, &c->inv, &c->phase, &c->phik, &c->chik, &c->fill,
-                    &c->Rocc, &c->Rchi, &c->Rgrad, &c->dens, &c->occfill, &c->Vloc, &c->dnu, &c->dnuT,
+                    &c->Rocc, &c->Rchi, &c->Rgrad, &c->dens, &c->densT, &c->occfill, &c->Vloc, &c->dnu, &c->dnuT,
                     &c->V3a1, &c->V3b1, &c->V3a2, &c->V3b2, &c->Qt, &c->Bt, &c->accP, &c->qtg, &c->div3b6,
                     &c->psi, &c->h2, &c->h3, &c->Rpsi, &c->Rgpsi, &c->acc2, &c->acc3, &c->qsum, &c->tmp,
                     &c->tmp2, &c->aux, &c->items, &c->meta};

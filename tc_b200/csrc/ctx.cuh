@@ -102,6 +102,7 @@ struct tcg_ctx {
     tcg::DBuf fill;                         // [nspin][nk][nbands] doubles
     tcg::DBuf Rocc, Rchi, Rgrad;            // R-space occupied grids (compute precision)
     tcg::DBuf dens;                         // [2][N] double2
+    tcg::DBuf densT;                        // [3][N] compute precision: n_0, n_1, n_0 + n_1
     tcg::DBuf occfill;                      // [nocc_grids] doubles: filling of each occupied grid
     // local three-body potentials built per state
     tcg::DBuf Vloc;                         // [nspin][N] double2 (tc3a1 + tc3b1 + ...)

@@ -308,6 +308,58 @@ __global__ void __launch_bounds__(128, Op::ZMINB) k_z_fast(Op op)
     }
 }
 
+// Z pass variant with one thread per z-line (ZL groups of 32 pencils split
+// the inputs / outputs); used by the terms whose G-space combination is
+// light (tc2x, band part of tc3a2a4b2b5), where it measured faster.
+constexpr int ZL = 4;
+template <typename T, int N, class Op>
+__global__ void __launch_bounds__(32 * ZL, Op::ZMINB) k_z_line(Op op)
+{
+    using V = typename C2<T>::t;
+    constexpr int TC = 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    V *S = tw + 128;                      // [NF][N][TC]
+    stage_tw<V>(op.g, tw, N);
+    __syncthreads();
+    const int item = blockIdx.y;
+    const int lane = threadIdx.x % TC, h = threadIdx.x / TC;
+    const int c = blockIdx.x * TC + lane;
+    const bool act = c < N * N;
+    const int x = c % N, y = c / N;
+    V v[N];
+    for (int f = h; f < Op::NF; f += ZL) {
+        if (act) {
+            const V *src = op.zin_grid(item, f) + c;
+#pragma unroll
+            for (int z = 0; z < N; z++) v[z] = src[(size_t)z * N * N];
+        } else {
+#pragma unroll
+            for (int z = 0; z < N; z++) v[z] = czero<V>();
+        }
+        line_fft<V, N, -1>(v, tw);
+        V *st = S + f * N * TC + lane;
+#pragma unroll
+        for (int z = 0; z < N; z++) st[z * TC] = v[z];
+    }
+    __syncthreads();
+    for (int o = h; o < Op::NB; o += ZL) {
+#pragma unroll
+        for (int z = 0; z < N; z++) {
+            V vin[Op::NF];
+#pragma unroll
+            for (int f = 0; f < Op::NF; f++) vin[f] = S[f * N * TC + z * TC + lane];
+            v[z] = act ? op.zmix(item, o, x, y, z, vin) : czero<V>();
+        }
+        if (Op::ZINV) line_fft<V, N, +1>(v, tw);
+        if (act) {
+            V *dst = op.out_grid(item, o) + c;
+#pragma unroll
+            for (int z = 0; z < N; z++) dst[(size_t)z * N * N] = v[z];
+        }
+    }
+}
+
 // ---------------------------------------------------------------- XYI ----
 // smem: twiddles + GS planes-of-P (results of a group) + 1 work set
 template <typename T, int N, class Op>

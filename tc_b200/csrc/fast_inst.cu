@@ -9,6 +9,10 @@
 namespace tcg {
 template <typename T> using OpQPBitc = OpQP<T, true>;
 template <typename T> using OpQPTc = OpQP<T, false>;
+template <typename T> using OpQPBitcEq = OpQP<T, true, true>;
+template <typename T> using OpQPTcEq = OpQP<T, false, true>;
+template <typename T> using OpTC3AEq = OpTC3A<T, true>;
+template <typename T> using OpTC3BEq = OpTC3B<T, true>;
 #define TCG_INST(T, OP) \
     template int run_chunk_fast<T, TCG_FAST_N, OP>(tcg_ctx *, const OP &, int, int, bool, bool);
 #define TCG_INST_ALL(T)                \
@@ -20,7 +24,11 @@ template <typename T> using OpQPTc = OpQP<T, false>;
     TCG_INST(T, OpPairFwd<T>)          \
     TCG_INST(T, OpBand<T>)             \
     TCG_INST(T, OpQPBitc<T>)           \
-    TCG_INST(T, OpQPTc<T>)
+    TCG_INST(T, OpQPTc<T>)             \
+    TCG_INST(T, OpQPBitcEq<T>)         \
+    TCG_INST(T, OpQPTcEq<T>)           \
+    TCG_INST(T, OpTC3AEq<T>)           \
+    TCG_INST(T, OpTC3BEq<T>)
 TCG_INST_ALL(float)
 TCG_INST_ALL(double)
 } // namespace tcg

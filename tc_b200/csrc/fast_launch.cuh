@@ -17,8 +17,14 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
         TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * Op::NF * gb, fast::k_xyf_fast<T, N, Op>,
                           dim3((np_f + CF::P - 1) / CF::P), dim3(CF::THREADS), fast::smem_xy_fast<V, N>(1), op, np_f));
     constexpr int TC = fast::zcols<V>();
-    TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb, fast::k_z_fast<T, N, Op>,
-                      dim3((N * N + TC - 1) / TC, items), dim3(128), fast::smem_z_fast<V, N>(Op::NF), op));
+    if constexpr (Op::ZSPLIT)
+        TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb,
+                          fast::k_z_fast<T, N, Op>, dim3((N * N + TC - 1) / TC, items), dim3(128),
+                          fast::smem_z_fast<V, N>(Op::NF), op));
+    else
+        TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb,
+                          fast::k_z_line<T, N, Op>, dim3((N * N + TC - 1) / TC, items), dim3(32 * fast::ZL),
+                          fast::smem_z_fast<V, N>(Op::NF), op));
     if (do_xyi) {
         const int nref = Op::REFWD ? Op::NB - 1 : 0;
         TRY(launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (Op::NB + nref) * gb, fast::k_xyi_fast<T, N, Op>,

@@ -32,6 +32,13 @@ __global__ void k_to_prec(const double2 *src, typename C2<T>::t *dst, size_t n)
         dst[i] = from64<typename C2<T>::t>(src[i]);
 }
 
+template <typename T>
+static __global__ void k_dens_sum(int N, const double2 *dens, typename C2<T>::t *out)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x)
+        out[p] = from64<typename C2<T>::t>(cadd(dens[p], dens[(size_t)N + p]));
+}
+
 // acc[t] += fac * V(r) * phi_t(r)   (local potentials: tc3a1.cpp:101-112 etc.)
 template <typename T>
 __global__ void k_local(int N, const typename C2<T>::t *Rpsi, const double2 *V, double2 *acc)
@@ -706,6 +713,53 @@ static int run_tc2x(tcg_ctx *c, const Targets &Tg, double2 *acc)
     return TCG_OK;
 }
 
+// tc3a3b3b4b6 stages A (first q loop) and B (3b6), EQ: equal Jastrow channels
+template <typename T, bool EQ>
+static int tc3_stage_ab(tcg_ctx *c, const Targets &Tg, const TRange &TR, const Sources &S, int s, double b3, double b6,
+                        double2 *acc, double2 *qsum)
+{
+    using V = typename C2<T>::t;
+    using OA = OpTC3A<T, EQ>;
+    using OB = OpTC3B<T, EQ>;
+    const Host &h = c->h;
+    const size_t N = h.N;
+    const bool bitc = h.method == TCG_METHOD_BITC;
+    const V *dnuT = c->dnuT.as<V>() + (size_t)s * 3 * N;
+    const int nsl = OA::NB, n2 = OB::NF;
+    std::vector<ChunkPlan> plan;
+    TRY(plan_chunks(c, c->meta, TR.n, TR.key, TR.cartk, (int)S.key.size(), S.key, S.cartq,
+                    max_items_for(c, nsl + n2, sizeof(V)), min_targets(c), plan));
+    for (const ChunkPlan &p : plan) {
+        const size_t items = (size_t)p.nt * p.ns;
+        TRY(c->tmp.ensure(items * nsl * N * sizeof(V)));
+        TRY(c->tmp2.ensure(items * n2 * N * sizeof(V)));
+        TRY(gen_tables(c, p, TAB_U_SX, s));
+        OA a;
+        op_common<T>(c, a, p, nsl, 2);
+        a.Rpsi = c->Rpsi.as<V>() + (size_t)(TR.t0 + p.t0) * N;
+        a.Rocc = c->Rocc.as<V>() + (S.base + p.s0) * N;
+        a.Rchi = (bitc ? c->Rchi.as<V>() : c->Rocc.as<V>()) + (S.base + p.s0) * N;
+        a.dnu = dnuT;
+        a.densT = c->densT.as<V>() + (EQ ? 2 * N : 0);
+        a.acc = acc + (size_t)(TR.t0 + p.t0) * N;
+        a.qsum = qsum + (size_t)(TR.t0 + p.t0) * 3 * N;
+        a.fill = c->occfill.as<double>() + S.base + p.s0;
+        a.tmp2 = c->tmp2.as<V>();
+        a.s = s;
+        a.b3 = b3;
+        TRY((run_chunk<T, OA>(c, a, (int)items, p.nt)));
+        OB b;
+        op_common<T>(c, b, p, nsl, 2);
+        b.Rocc = a.Rocc;
+        b.acc = a.acc;
+        b.tmp2 = a.tmp2;
+        b.b6 = b6;
+        b.s = s;
+        TRY((run_chunk<T, OB>(c, b, (int)items, p.nt, false, true)));
+    }
+    return TCG_OK;
+}
+
 template <typename T>
 static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, double2 *acc)
 {
@@ -727,36 +781,9 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
         if (TR.n == 0) continue;
         const V *dnuT = c->dnuT.as<V>() + (size_t)s * 3 * N;
         // stages A + B
-        std::vector<ChunkPlan> plan;
-        TRY(plan_chunks(c, c->meta, TR.n, TR.key, TR.cartk, (int)S.key.size(), S.key, S.cartq,
-                        max_items_for(c, 13, sizeof(V)), min_targets(c), plan));
-        for (const ChunkPlan &p : plan) {
-            const size_t items = (size_t)p.nt * p.ns;
-            TRY(c->tmp.ensure(items * 7 * N * sizeof(V)));
-            TRY(c->tmp2.ensure(items * 6 * N * sizeof(V)));
-            TRY(gen_tables(c, p, TAB_U_SX, s));
-            OpTC3A<T> a;
-            op_common<T>(c, a, p, 7, 2);
-            a.Rpsi = c->Rpsi.as<V>() + (size_t)(TR.t0 + p.t0) * N;
-            a.Rocc = c->Rocc.as<V>() + (S.base + p.s0) * N;
-            a.Rchi = (bitc ? c->Rchi.as<V>() : c->Rocc.as<V>()) + (S.base + p.s0) * N;
-            a.dnu = dnuT;
-            a.dens = c->dens.as<double2>();
-            a.acc = acc + (size_t)(TR.t0 + p.t0) * N;
-            a.qsum = qsum + (size_t)(TR.t0 + p.t0) * 3 * N;
-            a.fill = c->occfill.as<double>() + S.base + p.s0;
-            a.tmp2 = c->tmp2.as<V>();
-            a.s = s;
-            a.b3 = b3;
-            TRY((run_chunk<T, OpTC3A<T>>(c, a, (int)items, p.nt)));
-            OpTC3B<T> b;
-            op_common<T>(c, b, p, 7, 2);
-            b.Rocc = a.Rocc;
-            b.acc = a.acc;
-            b.tmp2 = a.tmp2;
-            b.b6 = b6;
-            TRY((run_chunk<T, OpTC3B<T>>(c, b, (int)items, p.nt, false, true)));
-        }
+        const bool eq = h.A[0 * 2 + s] == h.A[1 * 2 + s] && h.F[0 * 2 + s] == h.F[1 * 2 + s];
+        if (eq) TRY((tc3_stage_ab<T, true>(c, Tg, TR, S, s, b3, b6, acc, qsum)));
+        else TRY((tc3_stage_ab<T, false>(c, Tg, TR, S, s, b3, b6, acc, qsum)));
         // 3a3: acc += a3 sum_d qsum_d dnu_d  (:629-641)
         TRY(launch(c, k_dot3<T>, dim3((unsigned)((N + 255) / 256), TR.n), dim3(256), 0, (int)N,
                    (const double2 *)(qsum + (size_t)TR.t0 * 3 * N), dnuT, acc + (size_t)TR.t0 * N, a3, TR.n));
@@ -789,6 +816,7 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
             TCG_CUDA(cudaStreamSynchronize(c->stream));
         }
         // stage C: 3b4 (:651-770)
+        std::vector<ChunkPlan> plan;
         TRY(plan_chunks(c, c->meta, TR.n, TR.key, TR.cartk, (int)S.key.size(), S.key, S.cartq,
                         max_items_for(c, 3, sizeof(V)), min_targets(c), plan));
         for (const ChunkPlan &p : plan) {
@@ -805,6 +833,39 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
             op.b4 = b4;
             TRY((run_chunk<T, OpTC3C<T>>(c, op, (int)items, p.nt)));
         }
+    }
+    return TCG_OK;
+}
+
+// occupied-pair chunks of tc3a2a4b2b5 for spin sq
+template <typename T, bool BITC, bool EQ>
+static int qp_pairs(tcg_ctx *c, int sq, int ntq, const std::vector<int> &tkey, const std::vector<double> &tcart,
+                    const Sources &S, double2 *accP, int nacc)
+{
+    using V = typename C2<T>::t;
+    using OQ = OpQP<T, BITC, EQ>;
+    const Host &h = c->h;
+    const size_t N = h.N;
+    const int nsl = OQ::NB;
+    std::vector<ChunkPlan> plan;
+    TRY(plan_chunks(c, c->meta, ntq, tkey, tcart, (int)S.key.size(), S.key, S.cartq, max_items_for(c, nsl, sizeof(V)),
+                    min_targets(c), plan));
+    for (const ChunkPlan &p : plan) {
+        const size_t items = (size_t)p.nt * p.ns;
+        TRY(c->tmp.ensure(items * nsl * N * sizeof(V)));
+        TRY(gen_tables(c, p, TAB_U_QX, sq));
+        OQ op;
+        op_common<T>(c, op, p, nsl, 2);
+        op.Rq2 = c->qtg.as<V>() + (size_t)p.t0 * N;
+        op.Rq2c = BITC ? c->qtg.as<V>() + (size_t)(ntq + p.t0) * N : op.Rq2;
+        op.Rocc = c->Rocc.as<V>() + (S.base + p.s0) * N;
+        op.Rchi = (BITC ? c->Rchi.as<V>() : c->Rocc.as<V>()) + (S.base + p.s0) * N;
+        op.acc = accP + (size_t)p.t0 * nacc * N;
+        op.fill = c->occfill.as<double>() + S.base + p.s0;
+        op.nacc = nacc;
+        op.nspin = h.nspin;
+        op.sq = sq;
+        TRY((run_chunk<T, OQ>(c, op, (int)items, p.nt)));
     }
     return TCG_OK;
 }
@@ -866,42 +927,11 @@ static int qp_stage(tcg_ctx *c)
         TRY(c->accP.ensure((size_t)ntq * nacc * N * sizeof(double2)));
         double2 *accP = c->accP.as<double2>();
         TRY(launch(c, k_zero, dim3(148 * 8), dim3(256), 0, accP, (size_t)ntq * nacc * N));
-        std::vector<ChunkPlan> plan;
-        const int nsl = bitc ? 12 : 6;
-        TRY(plan_chunks(c, c->meta, ntq, tkey, tcart, (int)S.key.size(), S.key, S.cartq,
-                        max_items_for(c, nsl, sizeof(V)), min_targets(c), plan));
-        for (const ChunkPlan &p : plan) {
-            const size_t items = (size_t)p.nt * p.ns;
-            TRY(c->tmp.ensure(items * nsl * N * sizeof(V)));
-            TRY(gen_tables(c, p, TAB_U_QX, sq));
-            if (bitc) {
-                OpQP<T, true> op;
-                op_common<T>(c, op, p, nsl, 2);
-                op.Rq2 = c->qtg.as<V>() + (size_t)p.t0 * N;
-                op.Rq2c = c->qtg.as<V>() + (size_t)(ntq + p.t0) * N;
-                op.Rocc = c->Rocc.as<V>() + (S.base + p.s0) * N;
-                op.Rchi = c->Rchi.as<V>() + (S.base + p.s0) * N;
-                op.acc = accP + (size_t)p.t0 * nacc * N;
-                op.fill = c->occfill.as<double>() + S.base + p.s0;
-                op.nacc = nacc;
-                op.nspin = ns;
-                op.sq = sq;
-                TRY((run_chunk<T, OpQP<T, true>>(c, op, (int)items, p.nt)));
-            } else {
-                OpQP<T, false> op;
-                op_common<T>(c, op, p, nsl, 2);
-                op.Rq2 = c->qtg.as<V>() + (size_t)p.t0 * N;
-                op.Rq2c = op.Rq2;
-                op.Rocc = c->Rocc.as<V>() + (S.base + p.s0) * N;
-                op.Rchi = c->Rocc.as<V>() + (S.base + p.s0) * N;
-                op.acc = accP + (size_t)p.t0 * nacc * N;
-                op.fill = c->occfill.as<double>() + S.base + p.s0;
-                op.nacc = nacc;
-                op.nspin = ns;
-                op.sq = sq;
-                TRY((run_chunk<T, OpQP<T, false>>(c, op, (int)items, p.nt)));
-            }
-        }
+        const bool eqq = h.A[sq * 2 + 0] == h.A[sq * 2 + 1] && h.F[sq * 2 + 0] == h.F[sq * 2 + 1];
+        if (bitc && eqq) TRY((qp_pairs<T, true, true>(c, sq, ntq, tkey, tcart, S, accP, nacc)));
+        else if (bitc) TRY((qp_pairs<T, true, false>(c, sq, ntq, tkey, tcart, S, accP, nacc)));
+        else if (eqq) TRY((qp_pairs<T, false, true>(c, sq, ntq, tkey, tcart, S, accP, nacc)));
+        else TRY((qp_pairs<T, false, false>(c, sq, ntq, tkey, tcart, S, accP, nacc)));
         // B = -conj(Q) for TC, then forward FFTs of all accumulators
         if (!bitc)
             for (int i = 0; i < ntq; i++)
@@ -1146,6 +1176,11 @@ static int state_terms(tcg_ctx *c)
         std::vector<void *> gr{nG.as<double2>(), nG.as<double2>() + N};
         TRY((fft3_list<double, -1>(c, gr)));
     }
+    // compute-precision density [n_0, n_1, n_0 + n_1] (3b6 re-forward of tc3a3b3b4b6)
+    TRY(c->densT.ensure(3 * N * sizeof(V)));
+    TRY(launch(c, k_to_prec<T>, dim3(pblocks), dim3(256), 0, (const double2 *)c->dens.as<double2>(), c->densT.as<V>(), 2 * N));
+    TRY(launch(c, k_dens_sum<T>, dim3(pblocks), dim3(256), 0, (int)N, (const double2 *)c->dens.as<double2>(),
+               c->densT.as<V>() + 2 * N));
     TRY(c->dnu.ensure((size_t)ns * 3 * N * sizeof(double2)));
     TRY(c->dnuT.ensure((size_t)ns * 3 * N * sizeof(V)));
     TRY(c->V3a1.ensure((size_t)ns * N * sizeof(double2)));

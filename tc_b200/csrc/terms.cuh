@@ -169,6 +169,7 @@ struct OpBase {
     static constexpr bool ZINV = true, REFWD = false;
     static constexpr int GS = 1;
     static constexpr int ZMINB = 3;          // min resident CTAs of the fast Z pass (register cap)
+    static constexpr bool ZSPLIT = true;     // fast Z pass: z-lines split over lane pairs
     GridDesc g;
     V *tmp;
     int nsl;                // tmp slots per item
@@ -243,6 +244,7 @@ template <typename T>
 struct OpTC2X : OpBase<T> {
     using V = typename C2<T>::t;
     static constexpr const char *NAME = "tc2x";
+    static constexpr bool ZSPLIT = false;     // one thread per z-line measured faster here
     static constexpr bool REGACC = true;
     __device__ bool regacc_grid(int) const { return true; }
     __device__ V xyi_term(int, int item, int b, size_t p, const V *v) const
@@ -317,27 +319,25 @@ static __global__ void k_tables(GridDesc g, RecipC rc, Jastrow J, int mode, int 
 }
 
 // ======================================================= tc3a3b3b4b6 ops ==
-// stage A: first q loop (tc3a3b3b4b6.cpp:192-368)
-template <typename T>
+// stage A: first q loop (tc3a3b3b4b6.cpp:192-368).
+// EQ: u(G; 0, s) == u(G; 1, s) (same Jastrow A, F for both spins of x2), so
+// the spin sum of the 3b6 chain collapses by linearity,
+//   sum_x du_d FFT[n_x IFFT[phiphi du_d]] = du_d FFT[(n_0 + n_1) IFFT[phiphi du_d]],
+// and only three P grids (x = s) are needed instead of six.
+template <typename T, bool EQ = false>
 struct OpTC3A : OpBase<T> {
     using V = typename C2<T>::t;
     static constexpr const char *NAME = "3a3b6A";
-    static constexpr bool REGACC = false;   // register pressure outweighs the saved RMW here
-    __device__ bool regacc_grid(int b) const { return b == 0; }
-    __device__ V xyi_term(int, int item, int, size_t p, const V *v) const
-    {
-        const int si = item % this->ns;
-        return cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p])), (decltype(v[0].x))(fill[si] * b3));
-    }
-    __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
-    static constexpr int NF = 4, NB = 7;
+    static constexpr int NX = EQ ? 1 : 2;     // spin branches of x2 carried
+    static constexpr int NF = 4, NB = 1 + 3 * NX;
     static constexpr bool REFWD = true;
+    static constexpr bool REGACC = false;
     const V *Rpsi, *Rocc, *Rchi;  // [nt][N], [ns][N]
     const V *dnu;                 // [3][N] of the targets' spin
-    const double2 *dens;          // [2][N]
+    const V *densT;               // [2][N] density (EQ: [0] = n_0 + n_1), compute precision
     double2 *acc, *qsum;          // [nt][N], [nt][3][N]
     const double *fill;
-    V *tmp2;                      // [items][6][N]
+    V *tmp2;                      // [items][3 NX][N]
     int s;
     double b3;
     __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
@@ -362,7 +362,7 @@ struct OpTC3A : OpBase<T> {
             r = cadd(r, cscale(in[2], (S)(G[1] * u)));
             return cadd(r, cscale(in[3], (S)(G[2] * u)));
         }
-        const int xs = (o - 1) / 3, d = (o - 1) % 3;   // phiphi f du[xs]_d (:306-314)
+        const int xs = EQ ? s : (o - 1) / 3, d = (o - 1) % 3;   // phiphi f du[xs]_d (:306-314)
         const double f = fill[item % this->ns];
         return cscale(in[0], (S)(f * G[d] * tab[xs] * this->invN));
     }
@@ -374,24 +374,26 @@ struct OpTC3A : OpBase<T> {
         if (b == 0) {
             acc_red(acc + (size_t)tj * N + p, to64(cmul(v[0], phq)), fill[si] * b3);
         } else {
-            const int xs = (b - 1) / 3, d = (b - 1) % 3;
+            const int xs = EQ ? s : (b - 1) / 3, d = (b - 1) % 3;
             if (xs == s) acc_red(qsum + ((size_t)tj * 3 + d) * N + p, to64(cmul(v[0], phq)), 1.0);
         }
     }
     __device__ bool refwd_want(int b) const { return b > 0; }
     __device__ V refwd_load(int, int, int b, size_t p, V v) const
     {
-        const int xs = (b - 1) / 3;
-        return cmul(v, from64<V>(__ldg(&dens[(size_t)xs * this->g.N + p])));   // orbital * n_s2 (:332)
+        const int xs = EQ ? 0 : (b - 1) / 3;
+        return cmul(v, __ldg(&densT[(size_t)xs * this->g.N + p]));   // orbital * n_s2 (:332)
     }
-    __device__ V *refwd_grid(int item, int b) const { return tmp2 + ((size_t)item * 6 + (b - 1)) * this->g.N; }
+    __device__ V *refwd_grid(int item, int b) const { return tmp2 + ((size_t)item * 3 * NX + (b - 1)) * this->g.N; }
 };
 
 // stage B: [3b6] sum_{s2,d} FFT(.) du[s2]_d -> IFFT x phi_q (:333-348)
-template <typename T>
+template <typename T, bool EQ = false>
 struct OpTC3B : OpBase<T> {
     using V = typename C2<T>::t;
     static constexpr const char *NAME = "3b6B";
+    static constexpr int NX = EQ ? 1 : 2;
+    static constexpr int NF = 3 * NX, NB = 1;
     static constexpr bool REGACC = true;
     __device__ bool regacc_grid(int) const { return true; }
     __device__ V xyi_term(int, int item, int, size_t p, const V *v) const
@@ -400,12 +402,12 @@ struct OpTC3B : OpBase<T> {
         return cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p])), (decltype(v[0].x))b6);
     }
     __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
-    static constexpr int NF = 6, NB = 1;
     const V *Rocc;
     double2 *acc;
     V *tmp2;
     double b6;
-    __device__ V *zin_grid(int item, int f) const { return tmp2 + ((size_t)item * 6 + f) * this->g.N; }
+    int s;
+    __device__ V *zin_grid(int item, int f) const { return tmp2 + ((size_t)item * NF + f) * this->g.N; }
     __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
     {
         using S = decltype(in[0].x);
@@ -415,9 +417,11 @@ struct OpTC3B : OpBase<T> {
         const double *tab = this->tab_of(item) + 2 * p;
         V r = czero<V>();
 #pragma unroll
-        for (int xs = 0; xs < 2; xs++)
+        for (int xs = 0; xs < NX; xs++) {
+            const double u = tab[EQ ? s : xs] * this->invN;
 #pragma unroll
-            for (int d = 0; d < 3; d++) r = cadd(r, cscale(in[3 * xs + d], (S)(G[d] * tab[xs] * this->invN)));
+            for (int d = 0; d < 3; d++) r = cadd(r, cscale(in[3 * xs + d], (S)(G[d] * u)));
+        }
         return r;
     }
     __device__ void xyi_accum(int tj, int item, int, size_t p, const V *v) const
@@ -471,12 +475,16 @@ struct OpTC3C : OpBase<T> {
 };
 
 // ======================================================= tc3a2a4b2b5 ops ==
-// occupied-pair stage (tc3a2a4b2b5.cpp:210-443): targets (q2, i2), sources (q1, i1)
-template <typename T, bool BITC>
+// occupied-pair stage (tc3a2a4b2b5.cpp:210-443): targets (q2, i2), sources (q1, i1).
+// EQ: u(G; sq, 0) == u(G; sq, 1), so both branches x2 = 0, 1 give the same
+// orbital grids; one branch is transformed and its 3a2 contribution is
+// added to both spin slots (twice into slot 0 when unpolarised).
+template <typename T, bool BITC, bool EQ = false>
 struct OpQP : OpBase<T> {
     using V = typename C2<T>::t;
     static constexpr const char *NAME = "qp";
-    static constexpr int NF = BITC ? 2 : 1, NB = BITC ? 12 : 6, GS = BITC ? 2 : 1;
+    static constexpr int NX = EQ ? 1 : 2;
+    static constexpr int NF = BITC ? 2 : 1, NB = (BITC ? 6 : 3) * NX, GS = BITC ? 2 : 1;
     const V *Rq2, *Rq2c;          // targets phi_q2(r), chi_q2(r)  [nt][N]
     const V *Rocc, *Rchi;         // sources phi_q1, chi_q1        [ns][N]
     double2 *acc;                 // [nt][nacc][N]: 3a2[nspin], 3a4[3], 3b5[3]
@@ -499,6 +507,7 @@ struct OpQP : OpBase<T> {
         int xs, d, w;
         if (BITC) { w = o & 1; xs = (o >> 1) / 3; d = (o >> 1) % 3; }
         else { w = 0; xs = o / 3; d = o % 3; }
+        if (EQ) xs = sq;
         return cscale(in[w], (S)(G[d] * tab[xs] * this->invN));   // du[x]_d * phiphi (:378, :385)
     }
     __device__ void xyi_accum(int tj, int item, int b, size_t p, const V *v) const
@@ -509,20 +518,24 @@ struct OpQP : OpBase<T> {
         int xs, d;
         if (BITC) { xs = (b >> 1) / 3; d = (b >> 1) % 3; }
         else { xs = b / 3; d = b % 3; }
-        const int xr = nspin == 1 ? 0 : xs;
+        if (EQ) xs = sq;
         double2 *A = acc + (size_t)tj * nacc * N;
         const double2 o1 = to64(v[0]);
-        if (BITC) {
-            const double2 o2 = to64(v[1]);
-            acc_red(A + (size_t)xr * N + p, cmulc(o2, o1), -f1);                  // -f1 orbital conj(orbital2)
-            if (xs == sq) {
-                acc_red(A + (size_t)(nspin + d) * N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * N + p]))), f1);
-                const double2 cc = to64(cmul(cconj(v[1]), cconj(__ldg(&Rchi[(size_t)si * N + p]))));
+        const double2 c3a2 = BITC ? cmulc(to64(v[1]), o1) : double2{o1.x * o1.x + o1.y * o1.y, 0.0};
+        if (EQ) {
+            // both x2 branches: slot 0 twice (unpolarised) or slots 0 and 1
+            if (nspin == 1) acc_red(A + p, c3a2, -2.0 * f1);
+            else { acc_red(A + p, c3a2, -f1); acc_red(A + (size_t)N + p, c3a2, -f1); }
+        } else {
+            const int xr = nspin == 1 ? 0 : xs;
+            acc_red(A + (size_t)xr * N + p, c3a2, -f1);   // (:392-394 BITC, :404-406 TC)
+        }
+        if (xs == sq) {
+            acc_red(A + (size_t)(nspin + d) * N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * N + p]))), f1);
+            if (BITC) {
+                const double2 cc = to64(cmul(cconj(v[BITC ? 1 : 0]), cconj(__ldg(&Rchi[(size_t)si * N + p]))));
                 acc_red(A + (size_t)(nspin + 3 + d) * N + p, cc, -f1);               // (:428-430)
             }
-        } else {
-            acc_red(A + (size_t)xr * N + p, double2{o1.x * o1.x + o1.y * o1.y, 0.0}, -f1);   // (:404-406)
-            if (xs == sq) acc_red(A + (size_t)(nspin + d) * N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * N + p]))), f1);
         }
     }
 };
@@ -554,6 +567,7 @@ template <typename T>
 struct OpBand : OpBase<T> {
     using V = typename C2<T>::t;
     static constexpr const char *NAME = "band";
+    static constexpr bool ZSPLIT = false;     // one thread per z-line measured faster here
     static constexpr bool REGACC = true;
     __device__ bool regacc_grid(int) const { return true; }
     __device__ V xyi_term(int, int item, int b, size_t p, const V *v) const

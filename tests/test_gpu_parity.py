@@ -212,3 +212,31 @@ def test_gpu_matches_golden_fixture(name):
     for got, want in ((g2, ref["h2"]), (g3, ref["h3"])):
         if np.abs(want).max() > 0:
             assert rel(got, want) < FP64_TOL
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+@pytest.mark.parametrize("method", ["TC", "BITC"])
+def test_unequal_jastrow_channels(method, prec, tol):
+    """parallel / antiparallel Jastrow channels differ (cusp-like F): the
+    general spin-branch path of tc3a3b3b4b6 and tc3a2a4b2b5"""
+    A = np.array([[0.5, 0.7], [0.7, 0.5]])
+    F = np.array([[1.2, 0.9], [0.9, 1.2]])
+    s = synth.small(method, A=A, F=F, seed=5)
+    mask = abi.TERM_TC3A2A4B2B5 | abi.TERM_TC3A3B3B4B6
+    r2, r3 = O.apply(s, mask)
+    with Context(s, prec) as ctx:
+        ctx.set_state()
+        g2, g3 = ctx.apply(mask)
+    assert rel(g3, r3) < tol
+
+
+def test_unequal_channels_spin_polarised():
+    A = np.array([[0.5, 0.6], [0.6, 0.4]])
+    F = np.array([[1.0, 0.8], [0.8, 1.1]])
+    s = synth.small("BITC", A=A, F=F, nspin=2, seed=6)
+    r2, r3 = O.apply(s, abi.TERMS_TC)
+    with Context(s, "fp64") as ctx:
+        ctx.set_state()
+        g2, g3 = ctx.apply(abi.TERMS_TC)
+    assert rel(g2, r2) < FP64_TOL
+    assert rel(g3, r3) < FP64_TOL
