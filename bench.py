@@ -35,6 +35,12 @@ METRIC = "BITC H psi band-applies/s, mixed vs FP64 on one B200 at |dE|<=1e-6 Ha"
 UNIT = "band-applies/s"
 TERMS = ["tc2x", "tc3a1", "tc3b1", "tc3a2a4b2b5", "tc3a3b3b4b6"]
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+WORKLOADS = {
+    "C3": "BITC batched apply: fcc Si a=10.26, 4x4x4 MP (64 k), 14 Ha (645-692 PW/k), "
+          "grid 36^3, 16 bands/k (4 occ), all 5 TC terms + per-state work",
+    "C3s": "BITC batched apply, profiling case: fcc Si a=10.26, 2x2x2 MP (8 k), 14 Ha, "
+           "grid 36^3, 16 bands/k (4 occ), all 5 TC terms + per-state work",
+}
 
 
 def peaks():
@@ -196,10 +202,12 @@ def run_ours(args):
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.nvtx.range_push("bench_timed")   # ncu --nvtx-include "bench_timed]"
             e0.record(stream)
             ctx.refresh_state()
             ctx.apply_device(mask, psi_dev.data_ptr(), h2.data_ptr(), h3.data_ptr(), owned=owned)
             e1.record(stream)
+            torch.cuda.nvtx.range_pop()
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) / 1e3)
         clk = clocks.stop()
@@ -305,8 +313,7 @@ def run_ours(args):
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(step_s * 1e3, 2), "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "c64-fft/f64-acc", "data": "synthetic (seeded)",
-        "config": {"workload": "BITC batched apply: fcc Si a=10.26, 4x4x4 MP (64 k), 14 Ha (645-692 PW/k), "
-                               "grid 36^3, 16 bands/k (4 occ), all 5 TC terms + per-state work",
+        "config": {"workload": WORKLOADS.get(args.config, args.config),
                    "config": args.config, "band_applies_per_step": nb_total, "parallelism": f"k-shard{world}",
                    "l2": "flushed between timed steps (256 MiB write)"},
         "fp64": None if fp64 is None else {"value": round(nb_total * len(fp64["times"]) / t_fp64, 3),

@@ -187,6 +187,8 @@ extern "C" int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg
             if (h.n[0] == f) c->fast_n = f;
     }
     if (getenv("TCG_GENERIC_PASSES")) c->force_generic = true;
+    if (const char *e = getenv("TCG_XY_KERNELS"))   // "line" / "pair": override the per-term choice
+        c->xy_kernels = !strcmp(e, "line") ? 1 : (!strcmp(e, "pair") ? 2 : 0);
     *out = c;
     return TCG_OK;
 }

@@ -117,6 +117,7 @@ struct tcg_ctx {
     tcg::DBuf Rpsi, Rgpsi, acc2, acc3, qsum, tmp, tmp2, aux, items, meta;
     int fast_n = 0;                         // cubic grid size with compiled fast kernels (0: generic path)
     bool force_generic = false;             // use the generic pass kernels even if fast_n is set
+    int xy_kernels = 0;                     // fast XY passes: 0 per-term choice, 1 all line, 2 all lane-pair
     size_t tmp_budget = 0;                  // bytes per chunk of pass temporaries (0: default 1 GiB)
     int64_t launches = 0;
     // optional per-kernel timing with CUDA events on the context stream

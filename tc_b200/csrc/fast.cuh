@@ -15,6 +15,9 @@
 //            registers and stored.
 // Rows of a shared plane are padded to N+1 elements (odd stride for even N)
 // so that the row sweeps are free of bank conflicts.
+// Both XY passes also exist with each line split over a lane pair
+// (k_xyf_pair / k_xyi_pair: N/2 values per thread, one radix-2 step through
+// shuffles); each term picks one form per pass (Op::XYF_PAIR, Op::XYI_PAIR).
 #pragma once
 #include "fft.cuh"
 
@@ -382,11 +385,16 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2)
     // register accumulation only in the FP32 path (an FP64 column would
     // double the register footprint of the line FFT)
     constexpr bool RACC = Op::REGACC && sizeof(V) == 8;
+    // BOUT: one accumulator per output grid b (GS == 1); the b loop runs
+    // outside the source loop and each b's column sum is flushed on its own
+    constexpr bool BOUT = RACC && Op::BOUTER;
+    static_assert(!BOUT || Op::GS == 1, "per-output accumulation needs GS == 1");
     V racc[RACC ? N : 1];
+    for (int bo = 0; bo < (BOUT ? Op::NB : 1); bo++) {
 #pragma unroll
     for (int i = 0; i < (RACC ? N : 1); i++) racc[i] = czero<V>();
     for (int si = 0; si < ns; si++) {
-        for (int b0 = 0; b0 < Op::NB; b0 += Op::GS) {
+        for (int b0 = BOUT ? bo : 0; b0 < (BOUT ? bo + 1 : Op::NB); b0 += Op::GS) {
             V *keepc = W + PS + pl * N * PAD + ln;      // set 1, this thread's column
 #pragma unroll
             for (int q = 0; q < Op::GS; q++) {
@@ -444,6 +452,14 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2)
                     // derived plane: column values -> forward column FFT -> smem -> forward rows -> global
                     const bool want = op.refwd_want(b0);
                     if (want) {
+                        // per-output sums wait in this thread's own column of the
+                        // read set (no other thread touches it until the next
+                        // load), which frees their registers for the two FFTs
+                        V *stash = A + pl * N * PAD + ln;
+                        if constexpr (BOUT) {
+#pragma unroll
+                            for (int i = 0; i < N; i++) stash[i * PAD] = racc[i];
+                        }
                         const int item = op.item_of(tj, si);
 #pragma unroll
                         for (int yy = 0; yy < N; yy++)
@@ -472,15 +488,250 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2)
                                 op.refwd_grid(it, b0)[(size_t)(pid % N) * N * N + r] = B[qq * N * PAD + (r / N) * PAD + (r % N)];
                             }
                         }
+                        if constexpr (BOUT) {
+#pragma unroll
+                            for (int i = 0; i < N; i++) racc[i] = stash[i * PAD];
+                        }
                     }
                 }
             }
         }
     }
-    if (RACC && mine) {
+    if constexpr (BOUT) {
+        if (mine && op.regacc_grid(bo)) {
+#pragma unroll
+            for (int yy = 0; yy < N; yy++) op.xyi_flush_b(tj, bo, (size_t)z * N * N + (size_t)yy * N + ln, racc[yy]);
+        }
+    }
+    }
+    if (RACC && !BOUT && mine) {
 #pragma unroll
         for (int yy = 0; yy < N; yy++) op.xyi_flush(tj, (size_t)z * N * N + (size_t)yy * N + ln, racc[yy]);
     }
+}
+
+// ------------------------------------------------- XY passes, line pairs --
+// The same XY passes with each row / column split over a lane pair
+// (s = lane & 1, as in the Z pass): half the registers per thread, so twice
+// the warps stay resident.  Forward lines: natural halves x = s M + i in,
+// frequencies 2k + s out (fwd_split); inverse lines: frequencies 2k + s in,
+// natural halves out (inv_split).  Pairs are adjacent lanes, so a CTA holds
+// whole warps: P N is a multiple of 16.
+__host__ __device__ constexpr int gcd_c(int a, int b) { return b == 0 ? a : gcd_c(b, a % b); }
+template <int N, int VB> struct CfgP {
+    static constexpr int Q = 16 / gcd_c(N, 16);
+    static constexpr int P = (96 + Q * N - 1) / (Q * N) * Q;         // >= 96 lines per CTA
+    static constexpr int PAD = N + ((N % 2 == 0) ? 1 : 0);
+    static constexpr int THREADS = 2 * P * N;
+    // register cap: FP32 keeps >= 16 warps per SM, FP64 one CTA's worth
+    static constexpr int CTAS = VB == 8 ? (512 + THREADS - 1) / THREADS : 1;
+    static constexpr int REG0 = (65536 / (CTAS * THREADS)) & ~7;
+    static constexpr int REG = REG0 < 168 ? REG0 : 168;
+    static_assert(THREADS % 32 == 0, "line pairs need whole warps");
+};
+
+template <typename T, int N, class Op>
+__global__ void __launch_bounds__(CfgP<N, sizeof(typename C2<T>::t)>::THREADS)
+    __maxnreg__((CfgP<N, sizeof(typename C2<T>::t)>::REG)) k_xyf_pair(Op op, int nplanes)
+{
+    using V = typename C2<T>::t;
+    using CF = CfgP<N, sizeof(V)>;
+    constexpr int P = CF::P, PAD = CF::PAD, M = N / 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);   // [N]
+    V *twM = tw + 64;                          // [M]
+    V *A = tw + 128;
+    stage_tw<V>(op.g, tw, N);
+    __syncthreads();
+    for (int i = threadIdx.x; i < M; i += blockDim.x) twM[i] = tw[2 * i];
+    const int s = threadIdx.x & 1, pi = threadIdx.x >> 1;
+    const int pl = pi / N, ln = pi % N;
+    const int pid0 = blockIdx.x * P;
+    for (int f = 0; f < Op::NF; f++) {
+        __syncthreads();
+#pragma unroll 4
+        for (int k = 0; k < M; k++) {
+            const int e = threadIdx.x + k * CF::THREADS;
+            const int q = e / (N * N), r = e % (N * N);
+            const int pid = pid0 + q;
+            if (pid < nplanes) {
+                const int item = pid / N, z = pid % N, x = r % N, y = r / N;
+                A[q * N * PAD + y * PAD + x] = op.xyf_load(item, f, x, y, z, (size_t)z * N * N + r);
+            }
+        }
+        __syncthreads();
+        V v[M];
+        V *row = A + pl * N * PAD + ln * PAD;
+#pragma unroll
+        for (int i = 0; i < M; i++) v[i] = row[s * M + i];
+        fwd_split<V, N>(v, s, tw, twM);
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < M; k++) row[2 * k + s] = v[k];
+        __syncthreads();
+        const V *col = A + pl * N * PAD + ln;
+#pragma unroll
+        for (int i = 0; i < M; i++) v[i] = col[(s * M + i) * PAD];
+        fwd_split<V, N>(v, s, tw, twM);
+        const int pid = pid0 + pl;
+        if (pid < nplanes) {
+            const int item = pid / N, z = pid % N;
+            V *dst = op.tmp_grid(item, f) + (size_t)z * N * N + ln;
+#pragma unroll
+            for (int k = 0; k < M; k++) dst[(2 * k + s) * N] = v[k];
+        }
+    }
+}
+
+template <typename T, int N, class Op>
+__global__ void __launch_bounds__(CfgP<N, sizeof(typename C2<T>::t)>::THREADS)
+    __maxnreg__((CfgP<N, sizeof(typename C2<T>::t)>::REG)) k_xyi_pair(Op op, int nplanes)
+{
+    using V = typename C2<T>::t;
+    using CF = CfgP<N, sizeof(V)>;
+    constexpr int P = CF::P, PAD = CF::PAD, M = N / 2;
+    constexpr int PS = P * N * PAD;       // one set of P planes
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    V *twM = tw + 64;
+    V *W = tw + 128;                      // [2][P][N][PAD]: read set, keep / work set
+    stage_tw<V>(op.g, tw, N);
+    __syncthreads();
+    for (int i = threadIdx.x; i < M; i += blockDim.x) twM[i] = tw[2 * i];
+    const int s = threadIdx.x & 1, pi = threadIdx.x >> 1;
+    const int pl = pi / N, ln = pi % N;
+    const int pid0 = blockIdx.x * P;
+    const int mypid = pid0 + pl;
+    const bool mine = mypid < nplanes;
+    const int tj = mine ? mypid / N : 0, z = mypid % N;
+    // all planes of the CTA must belong to targets with the same source count
+    const int ns = op.nsrc(pid0 / N);
+    constexpr bool RACC = Op::REGACC && sizeof(V) == 8;
+    constexpr bool BOUT = RACC && Op::BOUTER;
+    static_assert(!BOUT || Op::GS == 1, "per-output accumulation needs GS == 1");
+    // this thread's rows y = s M + n of its column, as element offsets
+    const size_t pz = (size_t)z * N * N + ln + (size_t)s * M * N;
+    V racc[RACC ? M : 1];
+    for (int bo = 0; bo < (BOUT ? Op::NB : 1); bo++) {
+#pragma unroll
+        for (int i = 0; i < (RACC ? M : 1); i++) racc[i] = czero<V>();
+        for (int si = 0; si < ns; si++) {
+            for (int b0 = BOUT ? bo : 0; b0 < (BOUT ? bo + 1 : Op::NB); b0 += Op::GS) {
+                V *keepc = W + PS + pl * N * PAD + ln + s * M * PAD;   // set 1: this thread's half column
+#pragma unroll
+                for (int q = 0; q < Op::GS; q++) {
+                    V *A = W;
+                    __syncthreads();
+#pragma unroll 4
+                    for (int k = 0; k < M; k++) {
+                        const int e = threadIdx.x + k * CF::THREADS;
+                        const int qq = e / (N * N), r = e % (N * N);
+                        const int pid = pid0 + qq;
+                        if (pid < nplanes) {
+                            const int it = op.item_of(pid / N, si);
+                            cp_async_elem(A + qq * N * PAD + (r / N) * PAD + (r % N),
+                                          op.xyi_grid(it, b0 + q) + (size_t)(pid % N) * N * N + r);
+                        }
+                    }
+                    cp_async_wait_all();
+                    __syncthreads();
+                    V v[M];
+                    V *row = A + pl * N * PAD + ln * PAD;
+#pragma unroll
+                    for (int k = 0; k < M; k++) v[k] = row[2 * k + s];
+                    inv_split<V, N>(v, s, tw, twM);
+                    __syncwarp();
+#pragma unroll
+                    for (int i = 0; i < M; i++) row[s * M + i] = v[i];
+                    __syncthreads();
+                    V *colp = A + pl * N * PAD + ln;
+#pragma unroll
+                    for (int k = 0; k < M; k++) v[k] = colp[(2 * k + s) * PAD];
+                    inv_split<V, N>(v, s, tw, twM);            // v[n]: row y = s M + n
+                    if (Op::GS > 1 && q < Op::GS - 1) {
+#pragma unroll
+                        for (int i = 0; i < M; i++) keepc[i * PAD] = v[i];
+                    } else if (mine) {
+                        const int item = op.item_of(tj, si);
+                        if (RACC && op.regacc_grid(b0)) {
+#pragma unroll
+                            for (int i = 0; i < M; i++) {
+                                V vals[1] = {v[i]};
+                                racc[i] = cadd(racc[i], op.xyi_term(tj, item, b0, pz + (size_t)i * N, vals));
+                            }
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < M; i++) {
+                                V vals[Op::GS];
+                                if constexpr (Op::GS > 1) { vals[0] = keepc[i * PAD]; vals[Op::GS - 1] = v[i]; }
+                                else vals[0] = v[i];
+                                op.xyi_accum(tj, item, b0, pz + (size_t)i * N, vals);
+                            }
+                        }
+                    }
+                    if (Op::REFWD && Op::GS == 1) {
+                        const bool want = op.refwd_want(b0);   // uniform over the CTA
+                        if (want) {
+                            // the column sums wait in the slots this thread read
+                            V *stash = colp + s * PAD;
+                            if constexpr (BOUT) {
+#pragma unroll
+                                for (int k = 0; k < M; k++) stash[2 * k * PAD] = racc[k];
+                            }
+                            const int item = op.item_of(tj, si);
+#pragma unroll
+                            for (int i = 0; i < M; i++)
+                                v[i] = mine ? op.refwd_load(tj, item, b0, pz + (size_t)i * N, v[i]) : czero<V>();
+                            fwd_split<V, N>(v, s, tw, twM);          // frequencies y = 2k + s
+                            V *B = W + PS;
+                            V *cb = B + pl * N * PAD + ln;
+#pragma unroll
+                            for (int k = 0; k < M; k++) cb[(2 * k + s) * PAD] = v[k];
+                            __syncthreads();
+                            V *rb = B + pl * N * PAD + ln * PAD;
+#pragma unroll
+                            for (int i = 0; i < M; i++) v[i] = rb[s * M + i];
+                            fwd_split<V, N>(v, s, tw, twM);
+                            __syncwarp();
+#pragma unroll
+                            for (int k = 0; k < M; k++) rb[2 * k + s] = v[k];
+                            __syncthreads();
+#pragma unroll 4
+                            for (int k = 0; k < M; k++) {
+                                const int e = threadIdx.x + k * CF::THREADS;
+                                const int qq = e / (N * N), r = e % (N * N);
+                                const int pid = pid0 + qq;
+                                if (pid < nplanes) {
+                                    const int it = op.item_of(pid / N, si);
+                                    op.refwd_grid(it, b0)[(size_t)(pid % N) * N * N + r] =
+                                        B[qq * N * PAD + (r / N) * PAD + (r % N)];
+                                }
+                            }
+                            if constexpr (BOUT) {
+#pragma unroll
+                                for (int k = 0; k < M; k++) racc[k] = stash[2 * k * PAD];
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if constexpr (BOUT) {
+            if (mine && op.regacc_grid(bo)) {
+#pragma unroll
+                for (int i = 0; i < M; i++) op.xyi_flush_b(tj, bo, pz + (size_t)i * N, racc[i]);
+            }
+        }
+    }
+    if (RACC && !BOUT && mine) {
+#pragma unroll
+        for (int i = 0; i < M; i++) op.xyi_flush(tj, pz + (size_t)i * N, racc[i]);
+    }
+}
+
+template <typename V, int N> __host__ inline size_t smem_xy_pair(int sets)
+{
+    return sizeof(V) * (128 + (size_t)sets * CfgP<N, sizeof(V)>::P * N * CfgP<N, sizeof(V)>::PAD);
 }
 
 template <typename V, int N> __host__ inline size_t smem_xy_fast(int sets)

@@ -13,9 +13,17 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
     using CF = fast::Cfg<N, sizeof(V)>;
     const double gb = (double)N * N * N * sizeof(V);
     const int np_f = items * N, np_i = nt * N;
-    if (do_xyf)
-        TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * Op::NF * gb, fast::k_xyf_fast<T, N, Op>,
-                          dim3((np_f + CF::P - 1) / CF::P), dim3(CF::THREADS), fast::smem_xy_fast<V, N>(1), op, np_f));
+    using CP = fast::CfgP<N, sizeof(V)>;
+    const bool fpair = c->xy_kernels ? c->xy_kernels == 2 : Op::XYF_PAIR;
+    const bool ipair = c->xy_kernels ? c->xy_kernels == 2 : Op::XYI_PAIR;
+    if (do_xyf) {
+        if (!fpair)
+            TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * Op::NF * gb, fast::k_xyf_fast<T, N, Op>,
+                              dim3((np_f + CF::P - 1) / CF::P), dim3(CF::THREADS), fast::smem_xy_fast<V, N>(1), op, np_f));
+        else
+            TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * Op::NF * gb, fast::k_xyf_pair<T, N, Op>,
+                              dim3((np_f + CP::P - 1) / CP::P), dim3(CP::THREADS), fast::smem_xy_pair<V, N>(1), op, np_f));
+    }
     constexpr int TC = fast::zcols<V>();
     if constexpr (Op::ZSPLIT)
         TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb,
@@ -27,8 +35,12 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
                           fast::smem_z_fast<V, N>(Op::NF), op));
     if (do_xyi) {
         const int nref = Op::REFWD ? Op::NB - 1 : 0;
-        TRY(launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (Op::NB + nref) * gb, fast::k_xyi_fast<T, N, Op>,
-                          dim3((np_i + CF::P - 1) / CF::P), dim3(CF::THREADS), fast::smem_xy_fast<V, N>(2), op, np_i));
+        if (!ipair)
+            TRY(launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (Op::NB + nref) * gb, fast::k_xyi_fast<T, N, Op>,
+                              dim3((np_i + CF::P - 1) / CF::P), dim3(CF::THREADS), fast::smem_xy_fast<V, N>(2), op, np_i));
+        else
+            TRY(launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (Op::NB + nref) * gb, fast::k_xyi_pair<T, N, Op>,
+                              dim3((np_i + CP::P - 1) / CP::P), dim3(CP::THREADS), fast::smem_xy_pair<V, N>(2), op, np_i));
     }
     return TCG_OK;
 }

@@ -170,6 +170,9 @@ struct OpBase {
     static constexpr int GS = 1;
     static constexpr int ZMINB = 3;          // min resident CTAs of the fast Z pass (register cap)
     static constexpr bool ZSPLIT = true;     // fast Z pass: z-lines split over lane pairs
+    // fast XY passes: lines split over lane pairs (fewer registers, more warps,
+    // one shuffle per element and radix-2 step) or one thread per line
+    static constexpr bool XYF_PAIR = true, XYI_PAIR = false;
     GridDesc g;
     V *tmp;
     int nsl;                // tmp slots per item
@@ -194,6 +197,7 @@ struct OpBase {
     // contribute xyi_term(...) to a per-thread column sum flushed once per
     // chunk with xyi_flush; the other grids go through xyi_accum.
     static constexpr bool REGACC = false;
+    static constexpr bool BOUTER = false;    // one register accumulator per output grid (xyi_flush_b)
     __device__ bool regacc_grid(int) const { return false; }
     __device__ V xyi_term(int, int, int, size_t, const V *v) const { return v[0]; }
     __device__ void xyi_flush(int, size_t, V) const {}
@@ -331,7 +335,23 @@ struct OpTC3A : OpBase<T> {
     static constexpr int NX = EQ ? 1 : 2;     // spin branches of x2 carried
     static constexpr int NF = 4, NB = 1 + 3 * NX;
     static constexpr bool REFWD = true;
-    static constexpr bool REGACC = false;
+    static constexpr bool XYI_PAIR = true;   // the re-forward transforms need the register room
+    // FP32 column sums per output grid over the chunk's sources: b = 0 -> acc,
+    // b = 1 + 3 xs + d -> qsum[d] when xs == s (the other branch only re-forwards)
+    static constexpr bool REGACC = true, BOUTER = true;
+    __device__ bool regacc_grid(int b) const { return b == 0 || EQ || (b - 1) / 3 == s; }
+    __device__ V xyi_term(int, int item, int b, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        const V t = cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p]));
+        return b == 0 ? cscale(t, (decltype(t.x))(fill[si] * b3)) : t;
+    }
+    __device__ void xyi_flush_b(int tj, int b, size_t p, V sum) const
+    {
+        const size_t N = this->g.N;
+        if (b == 0) acc_red(acc + (size_t)tj * N + p, to64(sum), 1.0);
+        else acc_red(qsum + ((size_t)tj * 3 + (b - 1) % 3) * N + p, to64(sum), 1.0);
+    }
     const V *Rpsi, *Rocc, *Rchi;  // [nt][N], [ns][N]
     const V *dnu;                 // [3][N] of the targets' spin
     const V *densT;               // [2][N] density (EQ: [0] = n_0 + n_1), compute precision

@@ -8,6 +8,7 @@ here with numpy.random.default_rng(seed):
   C2  TC (tc2x + tc3*), same cell / k, RPA A=0.5 F=1.2, grid 32^3, 4 occ + 4 trial
   C3  BITC batched, 4x4x4 MP (64 k), 14 Ha, grid 36^3, 16 bands (4 occ),
       independent left / right orbitals, left bi-orthonormalised to right
+  C3s C3 on a 2x2x2 MP mesh (8 k): the reduced case for profiler captures
   C4  HEG, simple cubic, 54 e- at r_s = 2, Gamma only, 27 occupied plane-wave
       shells + 27 trial, 1e-3 seeded noise, grid 40^3
   C5  conventional cubic Si8 a=10.26, 3x3x3 MP (27 k), 20 Ha, grid 48^3,
@@ -290,6 +291,11 @@ def config(name, **over):
                   nbands=8, nocc=4, method="TC", seed=0, A=0.5, F=1.2)
     elif name == "C3":
         kw = dict(lattice=lattice_fcc(a), kvec_irr=mp_mesh(4), ecut=14.0, nr=(36, 36, 36),
+                  nbands=16, nocc=4, method="BITC", seed=2, left_seed=1, A=0.5, F=1.2)
+    elif name == "C3s":
+        # C3's cell, cutoff, grid, bands and Jastrow on a 2x2x2 mesh (8 k): the
+        # same kernels at an eighth of the k-points, small enough for ncu captures
+        kw = dict(lattice=lattice_fcc(a), kvec_irr=mp_mesh(2), ecut=14.0, nr=(36, 36, 36),
                   nbands=16, nocc=4, method="BITC", seed=2, left_seed=1, A=0.5, F=1.2)
     elif name == "C4":
         return heg_config(**over)

@@ -186,6 +186,21 @@ def test_generic_path_forced(monkeypatch):
     assert rel(g3, r3) < FP64_TOL
 
 
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+@pytest.mark.parametrize("xy", ["line", "pair"])
+@pytest.mark.parametrize("method", ["TC", "BITC"])
+def test_xy_kernel_forms(monkeypatch, method, xy, prec, tol):
+    """every term through both fast XY kernel forms (one thread per line, lane pairs)"""
+    monkeypatch.setenv("TCG_XY_KERNELS", xy)
+    s = system(method)
+    r2, r3 = oracle_terms(s, abi.TERMS_TC)
+    with Context(s, prec) as ctx:
+        ctx.set_state()
+        g2, g3 = ctx.apply(abi.TERMS_TC)
+    assert rel(g2, r2) < tol
+    assert rel(g3, r3) < tol
+
+
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_bitwise_deterministic(prec):
     """fixed-order accumulation: two applies give identical bits"""
