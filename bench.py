@@ -290,7 +290,9 @@ def run_ours(args):
     pk, pk_kind = peaks()
     # ---- roofline of the dominant kernel (pass tag with the most device time)
     prof = mixed["prof"] or {}
-    dom = max(((t, v) for t, v in prof.items() if t != "misc"), key=lambda x: x[1][1], default=None)
+    # pass kernels only: tags with algorithmic bytes (stage tags of small kernels carry none)
+    dom = max(((t, v) for t, v in prof.items() if v[2] > 0 and not t.startswith("idle>")),
+              key=lambda x: x[1][1], default=None)
     roof = None
     if dom is not None:
         tag, (cnt, ms, by) = dom
@@ -327,7 +329,9 @@ def run_ours(args):
         "e2e": e2e,
         "gpu_launches": mixed["launches"],
         "clocks": mixed["clocks"],
-        "profile": {t: {"launches": v[0], "ms": round(v[1], 3), "alg_GB": round(v[2] / 1e9, 3)} for t, v in prof.items()},
+        "profile": {t: {"launches": v[0], "ms": round(v[1], 3), "alg_GB": round(v[2] / 1e9, 3)} for t, v in prof.items()
+                    if not t.startswith("idle>")},
+        "idle_between_launches_ms": {t[5:]: round(v[1], 1) for t, v in prof.items() if t.startswith("idle>") and v[1] >= 1.0},
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(system, args.cpu_qstride)

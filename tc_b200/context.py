@@ -89,8 +89,9 @@ class Context:
         check(lib().tcg_profile(self.handle, 1 if enable else 0))
 
     def profile_read(self):
-        """{tag: (launches, device ms, algorithmic bytes)} of recorded launches."""
-        cap = 64
+        """{tag: (launches, device ms, algorithmic bytes)} of recorded launches; "idle>tag"
+        entries hold the device time between the previous launch and each launch of tag."""
+        cap = 128
         tags = C.create_string_buffer(32 * cap)
         cnt = (C.c_int64 * cap)()
         ms = (C.c_double * cap)()

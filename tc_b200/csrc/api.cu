@@ -189,6 +189,9 @@ extern "C" int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg
     if (getenv("TCG_GENERIC_PASSES")) c->force_generic = true;
     if (const char *e = getenv("TCG_XY_KERNELS"))   // "line" / "pair": override the per-term choice
         c->xy_kernels = !strcmp(e, "line") ? 1 : (!strcmp(e, "pair") ? 2 : 0);
+    if (getenv("TCG_XYI_NO_PREFETCH")) c->no_prefetch = true;
+    if (const char *e = getenv("TCG_Z_KERNELS"))    // "line" / "split": override the per-term choice
+        c->z_kernels = !strcmp(e, "line") ? 1 : (!strcmp(e, "split") ? 2 : 0);
     *out = c;
     return TCG_OK;
 }
@@ -201,7 +204,8 @@ extern "C" int tcg_ctx_destroy(tcg_ctx *c)
                     &c->Rocc, &c->Rchi, &c->Rgrad, &c->dens, &c->densT, &c->occfill, &c->Vloc, &c->dnu, &c->dnuT,
                     &c->V3a1, &c->V3b1, &c->V3a2, &c->V3b2, &c->Qt, &c->Bt, &c->accP, &c->qtg, &c->div3b6,
                     &c->psi, &c->h2, &c->h3, &c->Rpsi, &c->Rgpsi, &c->acc2, &c->acc3, &c->qsum, &c->tmp,
-                    &c->tmp2, &c->aux, &c->items, &c->meta};
+                    &c->tmp2, &c->aux, &c->ftab, &c->items, &c->meta, &c->rotw, &c->q3b2w,
+                    &c->nGw, &c->Ww};
     for (DBuf *b : bufs) b->release();
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -591,16 +595,27 @@ extern "C" int tcg_profile_read(tcg_ctx *c, int cap, char *tags /* cap x 32 */, 
     std::vector<std::string> names;
     std::vector<int64_t> cnt;
     std::vector<double> tms, tb;
-    for (auto &r : c->prof_recs) {
-        float e = 0;
-        TCG_CUDA(cudaEventElapsedTime(&e, r.a, r.b));
+    auto add = [&](const std::string &tag, double e, double by) {
         size_t i = 0;
         for (; i < names.size(); i++)
-            if (names[i] == r.tag) break;
-        if (i == names.size()) { names.push_back(r.tag); cnt.push_back(0); tms.push_back(0); tb.push_back(0); }
+            if (names[i] == tag) break;
+        if (i == names.size()) { names.push_back(tag); cnt.push_back(0); tms.push_back(0); tb.push_back(0); }
         cnt[i]++;
         tms[i] += e;
-        tb[i] += r.bytes;
+        tb[i] += by;
+    };
+    for (size_t k = 0; k < c->prof_recs.size(); k++) {
+        const auto &r = c->prof_recs[k];
+        float e = 0;
+        TCG_CUDA(cudaEventElapsedTime(&e, r.a, r.b));
+        add(r.tag, e, r.bytes);
+        if (k > 0) {
+            // device time between the previous launch's end and this one's start
+            // (host work, synchronisation, copies): reported as "idle>tag"
+            float gap = 0;
+            TCG_CUDA(cudaEventElapsedTime(&gap, c->prof_recs[k - 1].b, r.a));
+            add(std::string("idle>") + r.tag, gap, 0.0);
+        }
     }
     const int n = (int)std::min<size_t>(names.size(), (size_t)cap);
     for (int i = 0; i < n; i++) {

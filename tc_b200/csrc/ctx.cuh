@@ -115,9 +115,15 @@ struct tcg_ctx {
     // per-apply scratch
     tcg::DBuf psi, h2, h3;                  // packed fp64
     tcg::DBuf Rpsi, Rgpsi, acc2, acc3, qsum, tmp, tmp2, aux, items, meta;
+    tcg::DBuf rotw, q3b2w, nGw, Ww;           // per-state scratch kept across states (no per-step cudaMalloc / cudaFree)
+    tcg::DBuf ftab;                         // mixed path: FP32 G-space coefficient records of a chunk
+    int ftab_nrec = 1;
     int fast_n = 0;                         // cubic grid size with compiled fast kernels (0: generic path)
     bool force_generic = false;             // use the generic pass kernels even if fast_n is set
     int xy_kernels = 0;                     // fast XY passes: 0 per-term choice, 1 all line, 2 all lane-pair
+    bool no_prefetch = false;               // fast XYI: no prefetch of the next plane set
+    const char *stage = "misc";            // profiling tag of untagged launches (the current stage)
+    int z_kernels = 0;                      // fast Z pass: 0 per-term choice, 1 one thread per line, 2 lane pairs
     size_t tmp_budget = 0;                  // bytes per chunk of pass temporaries (0: default 1 GiB)
     int64_t launches = 0;
     // optional per-kernel timing with CUDA events on the context stream

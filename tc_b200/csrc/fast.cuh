@@ -158,16 +158,12 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 3)
     const int pid0 = blockIdx.x * P;
     for (int f = 0; f < Op::NF; f++) {
         __syncthreads();
-        // P*N*N elements, N per thread, loads batched by 4
+        // each thread fills column x = ln of its own plane (item and z fixed)
+        if (pid0 + pl < nplanes) {
+            const int item = (pid0 + pl) / N, z = (pid0 + pl) % N;
 #pragma unroll 4
-        for (int k = 0; k < N; k++) {
-            const int e = threadIdx.x + k * (P * N);
-            const int q = e / (N * N), r = e % (N * N);
-            const int pid = pid0 + q;
-            if (pid < nplanes) {
-                const int item = pid / N, z = pid % N, x = r % N, y = r / N;
-                A[q * N * PAD + y * PAD + x] = op.xyf_load(item, f, x, y, z, (size_t)z * N * N + r);
-            }
+            for (int k = 0; k < N; k++)
+                A[pl * N * PAD + k * PAD + ln] = op.xyf_load(item, f, ln, k, z, (size_t)z * N * N + (size_t)k * N + ln);
         }
         __syncthreads();
         V v[N];
@@ -401,16 +397,10 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2)
                 V *A = W;
                 __syncthreads();
                 // plane copies global -> smem without passing through registers
-#pragma unroll 4
-                for (int k = 0; k < N; k++) {
-                    const int e = threadIdx.x + k * (P * N);
-                    const int qq = e / (N * N), r = e % (N * N);
-                    const int pid = pid0 + qq;
-                    if (pid < nplanes) {
-                        const int it = op.item_of(pid / N, si);
-                        cp_async_elem(A + qq * N * PAD + (r / N) * PAD + (r % N),
-                                      op.xyi_grid(it, b0 + q) + (size_t)(pid % N) * N * N + r);
-                    }
+                if (mine) {   // column x = ln of this thread's own plane
+                    const V *src = op.xyi_grid(op.item_of(tj, si), b0 + q) + (size_t)z * N * N + ln;
+#pragma unroll
+                    for (int k = 0; k < N; k++) cp_async_elem(A + pl * N * PAD + k * PAD + ln, src + (size_t)k * N);
                 }
                 cp_async_wait_all();
                 __syncthreads();
@@ -478,15 +468,10 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2)
 #pragma unroll
                         for (int i = 0; i < N; i++) rb[i] = v[i];
                         __syncthreads();
-#pragma unroll
-                        for (int k = 0; k < N; k++) {
-                            const int e = threadIdx.x + k * (P * N);
-                            const int qq = e / (N * N), r = e % (N * N);
-                            const int pid = pid0 + qq;
-                            if (pid < nplanes) {
-                                const int it = op.item_of(pid / N, si);
-                                op.refwd_grid(it, b0)[(size_t)(pid % N) * N * N + r] = B[qq * N * PAD + (r / N) * PAD + (r % N)];
-                            }
+                        if (mine) {
+                            V *dstp = op.refwd_grid(op.item_of(tj, si), b0) + (size_t)z * N * N + ln;
+#pragma unroll 4
+                            for (int k = 0; k < N; k++) dstp[(size_t)k * N] = B[pl * N * PAD + k * PAD + ln];
                         }
                         if constexpr (BOUT) {
 #pragma unroll
@@ -505,6 +490,88 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2)
     }
     }
     if (RACC && !BOUT && mine) {
+#pragma unroll
+        for (int yy = 0; yy < N; yy++) op.xyi_flush(tj, (size_t)z * N * N + (size_t)yy * N + ln, racc[yy]);
+    }
+}
+
+// XYI with the next plane set prefetched: for terms without re-forwarded or
+// grouped grids (GS == 1, no REFWD) the two plane sets alternate, and the
+// asynchronous copies of step it + 1 (source, output grid) are in flight
+// while step it is transformed and accumulated.
+template <typename T, int N, class Op>
+__global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2) k_xyi_pf(Op op, int nplanes)
+{
+    using V = typename C2<T>::t;
+    static_assert(Op::GS == 1 && !Op::REFWD, "prefetching XYI handles plain outputs only");
+    constexpr int P = Cfg<N, sizeof(V)>::P, PAD = Cfg<N, sizeof(V)>::PAD;
+    constexpr int PS = P * N * PAD;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    V *W = tw + 128;                      // [2][P][N][PAD], alternating
+    stage_tw<V>(op.g, tw, N);
+    const int pl = threadIdx.x / N, ln = threadIdx.x % N;
+    const int pid0 = blockIdx.x * P;
+    const int mypid = pid0 + pl;
+    const bool mine = mypid < nplanes;
+    const int tj = mine ? mypid / N : 0, z = mypid % N;
+    const int ns = op.nsrc(pid0 / N);
+    constexpr bool RACC = Op::REGACC && sizeof(V) == 8;
+    V racc[RACC ? N : 1];
+#pragma unroll
+    for (int i = 0; i < (RACC ? N : 1); i++) racc[i] = czero<V>();
+    const int total = ns * Op::NB;        // steps: it = si * NB + b
+    auto issue = [&](int it) {
+        if (mine) {
+            const V *src = op.xyi_grid(op.item_of(tj, it / Op::NB), it % Op::NB) + (size_t)z * N * N + ln;
+            V *dst = W + (it & 1) * PS + pl * N * PAD + ln;
+#pragma unroll
+            for (int k = 0; k < N; k++) cp_async_elem(dst + k * PAD, src + (size_t)k * N);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    issue(0);
+    for (int it = 0; it < total; it++) {
+        __syncthreads();                  // every thread is done with the set that step it + 1 overwrites
+        if (it + 1 < total) {
+            issue(it + 1);
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        }
+        __syncthreads();
+        const int si = it / Op::NB, b0 = it % Op::NB;
+        V *A = W + (it & 1) * PS;
+        V v[N];
+        V *row = A + pl * N * PAD + ln * PAD;
+#pragma unroll
+        for (int i = 0; i < N; i++) v[i] = row[i];
+        line_fft<V, N, +1>(v, tw);
+#pragma unroll
+        for (int i = 0; i < N; i++) row[i] = v[i];
+        __syncthreads();
+        const V *colp = A + pl * N * PAD + ln;
+#pragma unroll
+        for (int i = 0; i < N; i++) v[i] = colp[i * PAD];
+        line_fft<V, N, +1>(v, tw);
+        if (mine) {
+            const int item = op.item_of(tj, si);
+            if (RACC && op.regacc_grid(b0)) {
+#pragma unroll
+                for (int yy = 0; yy < N; yy++) {
+                    V vals[1] = {v[yy]};
+                    racc[yy] = cadd(racc[yy], op.xyi_term(tj, item, b0, (size_t)z * N * N + (size_t)yy * N + ln, vals));
+                }
+            } else {
+#pragma unroll
+                for (int yy = 0; yy < N; yy++) {
+                    V vals[1] = {v[yy]};
+                    op.xyi_accum(tj, item, b0, (size_t)z * N * N + (size_t)yy * N + ln, vals);
+                }
+            }
+        }
+    }
+    if (RACC && mine) {
 #pragma unroll
         for (int yy = 0; yy < N; yy++) op.xyi_flush(tj, (size_t)z * N * N + (size_t)yy * N + ln, racc[yy]);
     }
@@ -549,14 +616,14 @@ __global__ void __launch_bounds__(CfgP<N, sizeof(typename C2<T>::t)>::THREADS)
     const int pid0 = blockIdx.x * P;
     for (int f = 0; f < Op::NF; f++) {
         __syncthreads();
-#pragma unroll 4
-        for (int k = 0; k < M; k++) {
-            const int e = threadIdx.x + k * CF::THREADS;
-            const int q = e / (N * N), r = e % (N * N);
-            const int pid = pid0 + q;
-            if (pid < nplanes) {
-                const int item = pid / N, z = pid % N, x = r % N, y = r / N;
-                A[q * N * PAD + y * PAD + x] = op.xyf_load(item, f, x, y, z, (size_t)z * N * N + r);
+        // the 2N threads of a plane fill it: element r0 + 2 k N, r0 = 2 ln + s
+        if (pid0 + pl < nplanes) {
+            const int item = (pid0 + pl) / N, z = (pid0 + pl) % N;
+            const int r0 = 2 * ln + s, x0 = r0 % N, y0 = r0 / N;
+#pragma unroll 6
+            for (int k = 0; k < M; k++) {
+                const int y = y0 + 2 * k;
+                A[pl * N * PAD + y * PAD + x0] = op.xyf_load(item, f, x0, y, z, (size_t)z * N * N + (size_t)y * N + x0);
             }
         }
         __syncthreads();
@@ -611,6 +678,8 @@ __global__ void __launch_bounds__(CfgP<N, sizeof(typename C2<T>::t)>::THREADS)
     static_assert(!BOUT || Op::GS == 1, "per-output accumulation needs GS == 1");
     // this thread's rows y = s M + n of its column, as element offsets
     const size_t pz = (size_t)z * N * N + ln + (size_t)s * M * N;
+    // plane copies: this thread moves elements r0 + 2 k N of its own plane
+    const int r0 = 2 * ln + s, x0 = r0 % N, y0 = r0 / N;
     V racc[RACC ? M : 1];
     for (int bo = 0; bo < (BOUT ? Op::NB : 1); bo++) {
 #pragma unroll
@@ -622,16 +691,11 @@ __global__ void __launch_bounds__(CfgP<N, sizeof(typename C2<T>::t)>::THREADS)
                 for (int q = 0; q < Op::GS; q++) {
                     V *A = W;
                     __syncthreads();
-#pragma unroll 4
-                    for (int k = 0; k < M; k++) {
-                        const int e = threadIdx.x + k * CF::THREADS;
-                        const int qq = e / (N * N), r = e % (N * N);
-                        const int pid = pid0 + qq;
-                        if (pid < nplanes) {
-                            const int it = op.item_of(pid / N, si);
-                            cp_async_elem(A + qq * N * PAD + (r / N) * PAD + (r % N),
-                                          op.xyi_grid(it, b0 + q) + (size_t)(pid % N) * N * N + r);
-                        }
+                    if (mine) {   // element r0 + 2 k N of this thread's own plane
+                        const V *src = op.xyi_grid(op.item_of(tj, si), b0 + q) + (size_t)z * N * N + (size_t)y0 * N + x0;
+                        V *dsm = A + pl * N * PAD + y0 * PAD + x0;
+#pragma unroll
+                        for (int k = 0; k < M; k++) cp_async_elem(dsm + 2 * k * PAD, src + (size_t)2 * k * N);
                     }
                     cp_async_wait_all();
                     __syncthreads();
@@ -696,16 +760,11 @@ __global__ void __launch_bounds__(CfgP<N, sizeof(typename C2<T>::t)>::THREADS)
 #pragma unroll
                             for (int k = 0; k < M; k++) rb[2 * k + s] = v[k];
                             __syncthreads();
-#pragma unroll 4
-                            for (int k = 0; k < M; k++) {
-                                const int e = threadIdx.x + k * CF::THREADS;
-                                const int qq = e / (N * N), r = e % (N * N);
-                                const int pid = pid0 + qq;
-                                if (pid < nplanes) {
-                                    const int it = op.item_of(pid / N, si);
-                                    op.refwd_grid(it, b0)[(size_t)(pid % N) * N * N + r] =
-                                        B[qq * N * PAD + (r / N) * PAD + (r % N)];
-                                }
+                            if (mine) {
+                                V *dstp = op.refwd_grid(op.item_of(tj, si), b0) + (size_t)z * N * N + (size_t)y0 * N + x0;
+                                const V *bs = B + pl * N * PAD + y0 * PAD + x0;
+#pragma unroll 6
+                                for (int k = 0; k < M; k++) dstp[(size_t)2 * k * N] = bs[2 * k * PAD];
                             }
                             if constexpr (BOUT) {
 #pragma unroll

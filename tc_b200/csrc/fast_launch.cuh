@@ -25,7 +25,8 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
                               dim3((np_f + CP::P - 1) / CP::P), dim3(CP::THREADS), fast::smem_xy_pair<V, N>(1), op, np_f));
     }
     constexpr int TC = fast::zcols<V>();
-    if constexpr (Op::ZSPLIT)
+    const bool zsplit = c->z_kernels ? c->z_kernels == 2 : Op::ZSPLIT;
+    if (zsplit)
         TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb,
                           fast::k_z_fast<T, N, Op>, dim3((N * N + TC - 1) / TC, items), dim3(128),
                           fast::smem_z_fast<V, N>(Op::NF), op));
@@ -35,6 +36,12 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
                           fast::smem_z_fast<V, N>(Op::NF), op));
     if (do_xyi) {
         const int nref = Op::REFWD ? Op::NB - 1 : 0;
+        if constexpr (Op::GS == 1 && !Op::REFWD) {
+            if (!ipair && !c->no_prefetch)
+                return launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (Op::NB + nref) * gb,
+                                     fast::k_xyi_pf<T, N, Op>, dim3((np_i + CF::P - 1) / CF::P), dim3(CF::THREADS),
+                                     fast::smem_xy_fast<V, N>(2), op, np_i);
+        }
         if (!ipair)
             TRY(launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (Op::NB + nref) * gb, fast::k_xyi_fast<T, N, Op>,
                               dim3((np_i + CF::P - 1) / CF::P), dim3(CF::THREADS), fast::smem_xy_fast<V, N>(2), op, np_i));

@@ -222,8 +222,16 @@ __global__ void __launch_bounds__(256) k_sphere_z(GridDesc g, const SphereItem *
 }
 
 // In-place XY pass over a list of grids (DIR = +1 backward, -1 forward).
+// Grid pointers of an in-place transform list: a device array, or up to 8
+// pointers passed by value (no upload, no synchronisation for short lists).
+struct GridRefs {
+    void *const *dev = nullptr;
+    void *inl[8] = {};
+    __device__ void *operator[](int i) const { return dev ? dev[i] : inl[i]; }
+};
+
 template <typename T, int DIR>
-__global__ void __launch_bounds__(256) k_xy_inplace(GridDesc g, void *const *grids)
+__global__ void __launch_bounds__(256) k_xy_inplace(GridDesc g, GridRefs grids)
 {
     using V = typename C2<T>::t;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -240,7 +248,7 @@ __global__ void __launch_bounds__(256) k_xy_inplace(GridDesc g, void *const *gri
 
 // In-place Z pass over a list of grids, result scaled by `scale`.
 template <typename T, int DIR>
-__global__ void __launch_bounds__(256) k_z_inplace(GridDesc g, void *const *grids, double scale)
+__global__ void __launch_bounds__(256) k_z_inplace(GridDesc g, GridRefs grids, double scale)
 {
     using V = typename C2<T>::t;
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -485,26 +485,39 @@ static void op_common(tcg_ctx *c, Op &op, const ChunkPlan &p, int nsl, int ntab)
     op.m.sb = p.sb;
     op.m.kq = p.kq;
     op.m.tab = c->aux.as<double>();
+    op.m.ftab = c->ftab.as<float4>();
     op.m.nSB = p.nSB;
     op.m.ntab = ntab;
+    op.m.nrec = c->ftab_nrec;
     memcpy(op.rc.R, c->h.recip, sizeof op.rc.R);
     op.invN = 1.0 / (double)c->h.N;
 }
 
-static int gen_tables(tcg_ctx *c, const ChunkPlan &p, int mode, int s)
+// Jastrow tables of one chunk: FP64 columns for the FP64 path, FP32
+// coefficient records (nrec per grid point) for the mixed path
+template <typename T>
+static int gen_tables(tcg_ctx *c, const ChunkPlan &p, int mode, int s, int nrec = 1)
 {
-    const int ntab = mode == TAB_U_SS ? 1 : 2;
     const int npair = p.nTB * p.nSB;
-    TRY(c->aux.ensure((size_t)npair * c->h.N * ntab * sizeof(double)));
     RecipC rc;
     memcpy(rc.R, c->h.recip, sizeof rc.R);
-    return launch(c, k_tables, dim3(148 * 4), dim3(256), 0, c->gd, rc, make_jastrow(c->h), mode, s, npair, p.kq,
-                  c->aux.as<double>());
+    if constexpr (sizeof(T) == 4) {
+        TRY(c->ftab.ensure((size_t)npair * c->h.N * nrec * sizeof(float4)));
+        c->ftab_nrec = nrec;
+        return launch(c, k_ftables, dim3(148 * 4), dim3(256), 0, c->gd, rc, make_jastrow(c->h), mode, s, nrec, npair,
+                      p.kq, 1.0 / (double)c->h.N, c->ftab.as<float4>());
+    } else {
+        const int ntab = mode == TAB_U_SS ? 1 : 2;
+        TRY(c->aux.ensure((size_t)npair * c->h.N * ntab * sizeof(double)));
+        return launch(c, k_tables, dim3(148 * 4), dim3(256), 0, c->gd, rc, make_jastrow(c->h), mode, s, npair, p.kq,
+                      c->aux.as<double>());
+    }
 }
 
 // forward transform + gather: h += fac * FFT(acc)
 static int finalize_acc(tcg_ctx *c, const Targets &T, double2 *acc, double2 *hout, double fac)
 {
+    PhaseScope ps_(c, "ap:final");
     const GridDesc &g = c->gd;
     const Host &h = c->h;
     const size_t nt = T.s.size();
@@ -527,8 +540,9 @@ static int finalize_acc(tcg_ctx *c, const Targets &T, double2 *acc, double2 *hou
     const int ntiles = (g.n0 * g.n1 + ZTC - 1) / ZTC;
     for (size_t b0 = 0; b0 < nt; b0 += 65535) {
         const unsigned nb = (unsigned)std::min<size_t>(65535, nt - b0);
-        TRY(launch(c, k_xy_inplace<double, -1>, dim3(g.n2, nb), dim3(256), smem_xy<double2>(g), g,
-                   (void *const *)(d_grids + b0)));
+        GridRefs gr;
+        gr.dev = d_grids + b0;
+        TRY(launch(c, k_xy_inplace<double, -1>, dim3(g.n2, nb), dim3(256), smem_xy<double2>(g), g, gr));
         TRY(launch(c, k_gather_z, dim3(ntiles, nb), dim3(256), smem_z<double2>(g, 0), g, (const GatherItem *)(d_gi + b0)));
     }
     TCG_CUDA(cudaStreamSynchronize(c->stream));
@@ -579,6 +593,7 @@ static size_t fill_off(const Host &h, int s, int k)
 
 static int div_2x(tcg_ctx *c, const Targets &T, const ApplyArgs &A, double2 *hout)
 {
+    PhaseScope ps_(c, "ap:div2x");
     const Host &h = c->h;
     if (!h.div) return TCG_OK;
     const size_t nt = T.s.size();
@@ -659,6 +674,7 @@ static TRange targets_of(const tcg_ctx *c, const Targets &T, int s)
 template <typename T>
 static int run_hf2x(tcg_ctx *c, const Targets &Tg, double2 *acc)
 {
+    PhaseScope ps_(c, "ap:2x");
     using V = typename C2<T>::t;
     const Host &h = c->h;
     const size_t N = h.N;
@@ -685,6 +701,7 @@ static int run_hf2x(tcg_ctx *c, const Targets &Tg, double2 *acc)
 template <typename T>
 static int run_tc2x(tcg_ctx *c, const Targets &Tg, double2 *acc)
 {
+    PhaseScope ps_(c, "ap:2x");
     using V = typename C2<T>::t;
     const Host &h = c->h;
     const size_t N = h.N;
@@ -697,7 +714,7 @@ static int run_tc2x(tcg_ctx *c, const Targets &Tg, double2 *acc)
                         max_items_for(c, 4, sizeof(V)), min_targets(c), plan));
         for (const ChunkPlan &p : plan) {
             TRY(c->tmp.ensure((size_t)p.nt * p.ns * 4 * N * sizeof(V)));
-            TRY(gen_tables(c, p, TAB_TC2X, s));
+            TRY(gen_tables<T>(c, p, TAB_TC2X, s));
             OpTC2X<T> op;
             op_common<T>(c, op, p, 4, 2);
             op.Rpsi = c->Rpsi.as<V>() + (size_t)(TR.t0 + p.t0) * N;
@@ -733,7 +750,7 @@ static int tc3_stage_ab(tcg_ctx *c, const Targets &Tg, const TRange &TR, const S
         const size_t items = (size_t)p.nt * p.ns;
         TRY(c->tmp.ensure(items * nsl * N * sizeof(V)));
         TRY(c->tmp2.ensure(items * n2 * N * sizeof(V)));
-        TRY(gen_tables(c, p, TAB_U_SX, s));
+        TRY(gen_tables<T>(c, p, TAB_U_SX, s, EQ ? 1 : 2));
         OA a;
         op_common<T>(c, a, p, nsl, 2);
         a.Rpsi = c->Rpsi.as<V>() + (size_t)(TR.t0 + p.t0) * N;
@@ -763,6 +780,7 @@ static int tc3_stage_ab(tcg_ctx *c, const Targets &Tg, const TRange &TR, const S
 template <typename T>
 static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, double2 *acc)
 {
+    PhaseScope ps_(c, "ap:tc3");
     using V = typename C2<T>::t;
     const Host &h = c->h;
     const size_t N = h.N;
@@ -822,7 +840,7 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
         for (const ChunkPlan &p : plan) {
             const size_t items = (size_t)p.nt * p.ns;
             TRY(c->tmp.ensure(items * 3 * N * sizeof(V)));
-            TRY(gen_tables(c, p, TAB_U_SS, s));
+            TRY(gen_tables<T>(c, p, TAB_U_SS, s));
             OpTC3C<T> op;
             op_common<T>(c, op, p, 3, 1);
             op.Rocc = c->Rocc.as<V>() + (S.base + p.s0) * N;
@@ -853,7 +871,7 @@ static int qp_pairs(tcg_ctx *c, int sq, int ntq, const std::vector<int> &tkey, c
     for (const ChunkPlan &p : plan) {
         const size_t items = (size_t)p.nt * p.ns;
         TRY(c->tmp.ensure(items * nsl * N * sizeof(V)));
-        TRY(gen_tables(c, p, TAB_U_QX, sq));
+        TRY(gen_tables<T>(c, p, TAB_U_QX, sq, EQ ? 1 : 2));
         OQ op;
         op_common<T>(c, op, p, nsl, 2);
         op.Rq2 = c->qtg.as<V>() + (size_t)p.t0 * N;
@@ -874,6 +892,7 @@ static int qp_pairs(tcg_ctx *c, int sq, int ntq, const std::vector<int> &tkey, c
 template <typename T>
 static int qp_stage(tcg_ctx *c)
 {
+    PhaseScope ps_(c, "st:qp");
     using V = typename C2<T>::t;
     Host &h = c->h;
     const size_t N = h.N;
@@ -892,9 +911,9 @@ static int qp_stage(tcg_ctx *c)
     TRY(c->V3b2.ensure((size_t)ns * N * sizeof(double2)));
     TRY(launch(c, k_zero, dim3(pblocks), dim3(256), 0, c->V3a2.as<double2>(), (size_t)ns * N));
     TRY(launch(c, k_zero, dim3(pblocks), dim3(256), 0, c->V3b2.as<double2>(), (size_t)ns * N));
-    DBuf rot;                         // fp64 work: 6 grids
+    DBuf &rot = c->rotw;              // fp64 work: 6 grids
     TRY(rot.ensure(6 * N * sizeof(double2)));
-    DBuf q3b2;
+    DBuf &q3b2 = c->q3b2w;
     TRY(q3b2.ensure(3 * N * sizeof(double2)));
     int rcode = TCG_OK;
     for (int sq = 0; sq < ns && rcode == TCG_OK; sq++) {
@@ -1061,8 +1080,6 @@ static int qp_stage(tcg_ctx *c)
         for (int s = 0; s < ns; s++) grids.push_back(c->V3a2.as<double2>() + (size_t)s * N);
         TRY((fft3_list<double, +1>(c, grids)));
     }
-    rot.release();
-    q3b2.release();
     TCG_CUDA(cudaStreamSynchronize(c->stream));
     h.qp_ready = true;
     return rcode;
@@ -1071,6 +1088,7 @@ static int qp_stage(tcg_ctx *c)
 template <typename T>
 static int run_tc3a2a4b2b5_band(tcg_ctx *c, const Targets &Tg, double2 *acc)
 {
+    PhaseScope ps_(c, "ap:band");
     using V = typename C2<T>::t;
     const Host &h = c->h;
     const size_t N = h.N;
@@ -1087,7 +1105,7 @@ static int run_tc3a2a4b2b5_band(tcg_ctx *c, const Targets &Tg, double2 *acc)
                         max_items_for(c, 4, sizeof(V)), min_targets(c), plan));
         for (const ChunkPlan &p : plan) {
             TRY(c->tmp.ensure((size_t)p.nt * p.ns * 4 * N * sizeof(V)));
-            TRY(gen_tables(c, p, TAB_U_SS, s));
+            TRY(gen_tables<T>(c, p, TAB_U_SS, s));
             OpBand<T> op;
             op_common<T>(c, op, p, 4, 1);
             op.Rpsi = c->Rpsi.as<V>() + (size_t)(TR.t0 + p.t0) * N;
@@ -1109,6 +1127,7 @@ static int run_tc3a2a4b2b5_band(tcg_ctx *c, const Targets &Tg, double2 *acc)
 template <typename T>
 static int build_occupied(tcg_ctx *c)
 {
+    PhaseScope ps_(c, "st:occupied");
     using V = typename C2<T>::t;
     Host &h = c->h;
     const bool bitc = h.method == TCG_METHOD_BITC;
@@ -1157,6 +1176,7 @@ static int build_occupied(tcg_ctx *c)
 template <typename T>
 static int state_terms(tcg_ctx *c)
 {
+    PhaseScope ps_(c, "st:local");
     using V = typename C2<T>::t;
     Host &h = c->h;
     h.qp_ready = false;
@@ -1169,7 +1189,7 @@ static int state_terms(tcg_ctx *c)
     memcpy(rc.R, h.recip, sizeof rc.R);
     const unsigned pblocks = (unsigned)std::min<size_t>(148 * 8, (N + 255) / 256);
     // density in G
-    DBuf nG;
+    DBuf &nG = c->nGw;
     TRY(nG.ensure(2 * N * sizeof(double2)));
     TCG_CUDA(cudaMemcpyAsync(nG.p, c->dens.p, 2 * N * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
     {
@@ -1185,7 +1205,7 @@ static int state_terms(tcg_ctx *c)
     TRY(c->dnuT.ensure((size_t)ns * 3 * N * sizeof(V)));
     TRY(c->V3a1.ensure((size_t)ns * N * sizeof(double2)));
     TRY(c->V3b1.ensure((size_t)ns * N * sizeof(double2)));
-    DBuf W;
+    DBuf &W = c->Ww;
     TRY(W.ensure((size_t)ns * 3 * N * sizeof(double2)));
     for (int s = 0; s < ns; s++) {
         double2 *dn = c->dnu.as<double2>() + (size_t)s * 3 * N;
@@ -1237,8 +1257,6 @@ static int state_terms(tcg_ctx *c)
             }
         }
     }
-    W.release();
-    nG.release();
     TCG_CUDA(cudaStreamSynchronize(c->stream));
     return TCG_OK;
 }
@@ -1247,6 +1265,7 @@ static int state_terms(tcg_ctx *c)
 template <typename T>
 static int apply_impl(tcg_ctx *c, const ApplyArgs &A)
 {
+    PhaseScope ps_(c, "ap:setup");
     using V = typename C2<T>::t;
     Host &h = c->h;
     const size_t N = h.N;

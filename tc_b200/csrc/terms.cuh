@@ -92,8 +92,9 @@ static int sphere_to_r(tcg_ctx *c, const std::vector<SphereItem> &items)
         const unsigned nb = (unsigned)std::min<size_t>(65535, n - b0);
         TRY(launch(c, k_sphere_z<T>, dim3(nz_tiles, nb), dim3(256), smem_z<V>(g, 0), g,
                    (const SphereItem *)(d_items + b0), c->recip.as<const double>()));
-        TRY(launch(c, k_xy_inplace<T, +1>, dim3(g.n2, nb), dim3(256), smem_xy<V>(g), g,
-                   (void *const *)(d_outs + b0)));
+        GridRefs gr;
+        gr.dev = d_outs + b0;
+        TRY(launch(c, k_xy_inplace<T, +1>, dim3(g.n2, nb), dim3(256), smem_xy<V>(g), g, gr));
     }
     TCG_CUDA(cudaStreamSynchronize(c->stream));   // c->items is reused by the next caller
     return TCG_OK;
@@ -107,18 +108,25 @@ static int fft3_list(tcg_ctx *c, const std::vector<void *> &grids)
     const GridDesc &g = c->gd;
     if (grids.empty()) return TCG_OK;
     const size_t n = grids.size();
+    const int ntiles = (g.n0 * g.n1 + ZTC - 1) / ZTC;
+    const double scale = DIR < 0 ? 1.0 / (double)g.N : 1.0;
+    if (n <= 8) {   // pointers by value: nothing to upload, nothing to wait for
+        GridRefs gr;
+        for (size_t i = 0; i < n; i++) gr.inl[i] = grids[i];
+        TRY(launch(c, k_xy_inplace<T, DIR>, dim3(g.n2, (unsigned)n), dim3(256), smem_xy<V>(g), g, gr));
+        return launch(c, k_z_inplace<T, DIR>, dim3(ntiles, (unsigned)n), dim3(256), smem_z<V>(g, 0), g, gr, scale);
+    }
     TRY(c->items.ensure(n * sizeof(void *)));
     void **d = c->items.as<void *>();
     TCG_CUDA(cudaMemcpyAsync(d, grids.data(), n * sizeof(void *), cudaMemcpyHostToDevice, c->stream));
-    const int ntiles = (g.n0 * g.n1 + ZTC - 1) / ZTC;
-    const double scale = DIR < 0 ? 1.0 / (double)g.N : 1.0;
     for (size_t b0 = 0; b0 < n; b0 += 65535) {
         const unsigned nb = (unsigned)std::min<size_t>(65535, n - b0);
-        TRY(launch(c, k_xy_inplace<T, DIR>, dim3(g.n2, nb), dim3(256), smem_xy<V>(g), g, (void *const *)(d + b0)));
-        TRY(launch(c, k_z_inplace<T, DIR>, dim3(ntiles, nb), dim3(256), smem_z<V>(g, 0), g, (void *const *)(d + b0),
-                   scale));
+        GridRefs gr;
+        gr.dev = d + b0;
+        TRY(launch(c, k_xy_inplace<T, DIR>, dim3(g.n2, nb), dim3(256), smem_xy<V>(g), g, gr));
+        TRY(launch(c, k_z_inplace<T, DIR>, dim3(ntiles, nb), dim3(256), smem_z<V>(g, 0), g, gr, scale));
     }
-    TCG_CUDA(cudaStreamSynchronize(c->stream));
+    TCG_CUDA(cudaStreamSynchronize(c->stream));   // c->items is reused by the next caller
     return TCG_OK;
 }
 
@@ -159,8 +167,9 @@ struct ChunkMeta {
     const int *tb;          // [nt]
     const int *sb;          // [ns]
     const double *kq;       // [nTB*nSB][3]
-    const double *tab;      // [nTB*nSB][N][ntab]
-    int nSB, ntab;
+    const double *tab;      // [nTB*nSB][N][ntab]            (FP64 path)
+    const float4 *ftab;     // [nTB*nSB][N][nrec] coefficients (mixed path)
+    int nSB, ntab, nrec;
 };
 
 template <typename T>
@@ -170,9 +179,10 @@ struct OpBase {
     static constexpr int GS = 1;
     static constexpr int ZMINB = 3;          // min resident CTAs of the fast Z pass (register cap)
     static constexpr bool ZSPLIT = true;     // fast Z pass: z-lines split over lane pairs
-    // fast XY passes: lines split over lane pairs (fewer registers, more warps,
-    // one shuffle per element and radix-2 step) or one thread per line
-    static constexpr bool XYF_PAIR = true, XYI_PAIR = false;
+    // fast XY passes: one thread per line (measured fastest for every term on
+    // 36^3 once the plane copies were made division-free) or lines split over
+    // lane pairs (half the registers, one shuffle per element)
+    static constexpr bool XYF_PAIR = false, XYI_PAIR = false;
     GridDesc g;
     V *tmp;
     int nsl;                // tmp slots per item
@@ -204,6 +214,14 @@ struct OpBase {
     __device__ int pair_id(int item) const { return m.tb[item / ns] * m.nSB + m.sb[item % ns]; }
     __device__ const double *kq_of(int item) const { return m.kq + 3 * pair_id(item); }
     __device__ const double *tab_of(int item) const { return m.tab + (size_t)pair_id(item) * g.N * m.ntab; }
+    // mixed path: record r of the coefficient table at grid point p
+    __device__ float4 fco(int item, size_t p, int r) const
+    {
+        return __ldg(&m.ftab[((size_t)pair_id(item) * g.N + p) * m.nrec + r]);
+    }
+    static constexpr bool FT = sizeof(T) == 4;   // mixed path: FP32 coefficient tables
+    __device__ static float comp(const float4 &c, int d) { return d == 0 ? c.x : (d == 1 ? c.y : (d == 2 ? c.z : c.w)); }
+    __device__ size_t pidx(int x, int y, int z) const { return (size_t)x + (size_t)g.n0 * (y + (size_t)g.n1 * z); }
 };
 
 // =================================================================== hf2x ==
@@ -275,6 +293,16 @@ struct OpTC2X : OpBase<T> {
     __device__ V zmix(int item, int o, int x, int y, int z, const V *in) const
     {
         using S = decltype(in[0].x);
+        if constexpr (OpBase<T>::FT) {
+            const float4 c = this->fco(item, this->pidx(x, y, z), 0);
+            if (o == 0) {
+                V r = cscale(in[0], c.x);
+                r = cadd(r, cscale(in[1], c.y));
+                r = cadd(r, cscale(in[2], c.z));
+                return cadd(r, cscale(in[3], c.w));
+            }
+            return cscale(in[0], this->comp(c, o));
+        }
         double G[3];
         gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
         const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
@@ -322,6 +350,42 @@ static __global__ void k_tables(GridDesc g, RecipC rc, Jastrow J, int mode, int 
     }
 }
 
+// FP32 coefficient tables of the mixed path, evaluated in FP64 and rounded
+// once; G = k - q + G_p, all include the 1/N of the forward transform:
+//   TAB_TC2X : {V_2body(s,s), G_0 u, G_1 u, G_2 u} / N       with u = u(G; s, s)
+//   TAB_U_SX : record r = {G_d u(G; x_r, s)} / N, x_r = r (nrec 2) or s (nrec 1)
+//   TAB_U_SS : {G_d u(G; s, s)} / N
+//   TAB_U_QX : record r = {G_d u(G; s, x_r)} / N, x_r = r (nrec 2) or s (nrec 1)
+static __global__ void k_ftables(GridDesc g, RecipC rc, Jastrow J, int mode, int s, int nrec, int npair,
+                                 const double *kq, double invN, float4 *tab)
+{
+    const size_t total = (size_t)npair * g.N;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int pr = (int)(i / g.N);
+        const size_t p = i % g.N;
+        int x, y, z;
+        xyz_of(g, p, x, y, z);
+        double G[3];
+        gvec(rc.R, g, x, y, z, kq + 3 * pr, G);
+        float4 *o = tab + i * nrec;
+        if (mode == TAB_TC2X) {
+            const double u = J.uk(G, s, s) * invN;
+            o[0] = make_float4((float)(J.tc2body(G, s, s) * invN), (float)(G[0] * u), (float)(G[1] * u),
+                               (float)(G[2] * u));
+            continue;
+        }
+        for (int r = 0; r < nrec; r++) {
+            const int xr = nrec == 1 ? s : r;
+            double u;
+            if (mode == TAB_U_SX) u = J.uk(G, xr, s);
+            else if (mode == TAB_U_QX) u = J.uk(G, s, xr);
+            else u = J.uk(G, s, s);
+            u *= invN;
+            o[r] = make_float4((float)(G[0] * u), (float)(G[1] * u), (float)(G[2] * u), 0.f);
+        }
+    }
+}
+
 // ======================================================= tc3a3b3b4b6 ops ==
 // stage A: first q loop (tc3a3b3b4b6.cpp:192-368).
 // EQ: u(G; 0, s) == u(G; 1, s) (same Jastrow A, F for both spins of x2), so
@@ -335,7 +399,7 @@ struct OpTC3A : OpBase<T> {
     static constexpr int NX = EQ ? 1 : 2;     // spin branches of x2 carried
     static constexpr int NF = 4, NB = 1 + 3 * NX;
     static constexpr bool REFWD = true;
-    static constexpr bool XYI_PAIR = true;   // the re-forward transforms need the register room
+    static constexpr bool ZSPLIT = false;    // one thread per z-line measured faster here
     // FP32 column sums per output grid over the chunk's sources: b = 0 -> acc,
     // b = 1 + 3 xs + d -> qsum[d] when xs == s (the other branch only re-forwards)
     static constexpr bool REGACC = true, BOUTER = true;
@@ -372,6 +436,18 @@ struct OpTC3A : OpBase<T> {
     __device__ V zmix(int item, int o, int x, int y, int z, const V *in) const
     {
         using S = decltype(in[0].x);
+        if constexpr (OpBase<T>::FT) {
+            const size_t p = this->pidx(x, y, z);
+            if (o == 0) {
+                const float4 c = this->fco(item, p, EQ ? 0 : s);
+                V r = cscale(in[1], c.x);
+                r = cadd(r, cscale(in[2], c.y));
+                return cadd(r, cscale(in[3], c.z));
+            }
+            const int xs = EQ ? s : (o - 1) / 3, d = (o - 1) % 3;
+            const float4 c = this->fco(item, p, EQ ? 0 : xs);
+            return cscale(in[0], (float)fill[item % this->ns] * this->comp(c, d));
+        }
         double G[3];
         gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
         const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
@@ -431,6 +507,18 @@ struct OpTC3B : OpBase<T> {
     __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
     {
         using S = decltype(in[0].x);
+        if constexpr (OpBase<T>::FT) {
+            const size_t p = this->pidx(x, y, z);
+            V r = czero<V>();
+#pragma unroll
+            for (int xs = 0; xs < NX; xs++) {
+                const float4 c = this->fco(item, p, xs);
+                r = cadd(r, cscale(in[3 * xs], c.x));
+                r = cadd(r, cscale(in[3 * xs + 1], c.y));
+                r = cadd(r, cscale(in[3 * xs + 2], c.z));
+            }
+            return r;
+        }
         double G[3];
         gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
         const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
@@ -479,6 +567,12 @@ struct OpTC3C : OpBase<T> {
     __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
     {
         using S = decltype(in[0].x);
+        if constexpr (OpBase<T>::FT) {
+            const float4 c = this->fco(item, this->pidx(x, y, z), 0);
+            V r = cscale(in[0], c.x);
+            r = cadd(r, cscale(in[1], c.y));
+            return cadd(r, cscale(in[2], c.z));
+        }
         double G[3];
         gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
         const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
@@ -520,6 +614,13 @@ struct OpQP : OpBase<T> {
     __device__ V zmix(int item, int o, int x, int y, int z, const V *in) const
     {
         using S = decltype(in[0].x);
+        if constexpr (OpBase<T>::FT) {
+            int xs, d, w;
+            if (BITC) { w = o & 1; xs = (o >> 1) / 3; d = (o >> 1) % 3; }
+            else { w = 0; xs = o / 3; d = o % 3; }
+            const float4 c = this->fco(item, this->pidx(x, y, z), EQ ? 0 : xs);
+            return cscale(in[w], this->comp(c, d));
+        }
         double G[3];
         gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
         const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
@@ -616,6 +717,13 @@ struct OpBand : OpBase<T> {
     __device__ V zmix(int item, int o, int x, int y, int z, const V *in) const
     {
         using S = decltype(in[0].x);
+        if constexpr (OpBase<T>::FT) {
+            const float4 c = this->fco(item, this->pidx(x, y, z), 0);
+            if (o < 3) return cscale(in[0], (float)(fill[item % this->ns] * fa4) * this->comp(c, o));
+            V r = cscale(in[1], c.x);
+            r = cadd(r, cscale(in[2], c.y));
+            return cadd(r, cscale(in[3], c.z));
+        }
         double G[3];
         gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
         const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);

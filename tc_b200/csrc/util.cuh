@@ -88,8 +88,16 @@ inline int launch_tagged(tcg_ctx *c, const char *tag, double alg_bytes, K kernel
 template <typename K, typename... Args>
 inline int launch(tcg_ctx *c, K kernel, dim3 grid, dim3 block, size_t smem, Args... args)
 {
-    return launch_tagged(c, "misc", 0.0, kernel, grid, block, smem, args...);
+    return launch_tagged(c, c->stage, 0.0, kernel, grid, block, smem, args...);
 }
+
+// Names the stage whose untagged launches follow (profiling only).
+struct PhaseScope {
+    tcg_ctx *c;
+    const char *old;
+    PhaseScope(tcg_ctx *c_, const char *name) : c(c_), old(c_->stage) { c->stage = name; }
+    ~PhaseScope() { c->stage = old; }
+};
 
 #define TRY(x)                     \
     do {                           \
