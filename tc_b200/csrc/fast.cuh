@@ -503,7 +503,7 @@ template <typename T, int N, class Op>
 __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2) k_xyi_pf(Op op, int nplanes)
 {
     using V = typename C2<T>::t;
-    static_assert(Op::GS == 1 && !Op::REFWD, "prefetching XYI handles plain outputs only");
+    static_assert(Op::GS == 1, "prefetching XYI handles ungrouped outputs only");
     constexpr int P = Cfg<N, sizeof(V)>::P, PAD = Cfg<N, sizeof(V)>::PAD;
     constexpr int PS = P * N * PAD;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -517,6 +517,7 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2)
     const int tj = mine ? mypid / N : 0, z = mypid % N;
     const int ns = op.nsrc(pid0 / N);
     constexpr bool RACC = Op::REGACC && sizeof(V) == 8;
+    static_assert(!(RACC && Op::REFWD), "re-forwarded outputs accumulate through xyi_accum");
     V racc[RACC ? N : 1];
 #pragma unroll
     for (int i = 0; i < (RACC ? N : 1); i++) racc[i] = czero<V>();
@@ -568,6 +569,31 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2)
                     V vals[1] = {v[yy]};
                     op.xyi_accum(tj, item, b0, (size_t)z * N * N + (size_t)yy * N + ln, vals);
                 }
+            }
+        }
+        if (Op::REFWD && op.refwd_want(b0)) {   // uniform over the CTA
+            // derived plane, transformed forward in place in the current set:
+            // columns (registers) -> own column -> rows -> global
+            __syncthreads();                      // every column of the set has been read
+            const int item = op.item_of(tj, si);
+#pragma unroll
+            for (int yy = 0; yy < N; yy++)
+                v[yy] = mine ? op.refwd_load(tj, item, b0, (size_t)z * N * N + (size_t)yy * N + ln, v[yy]) : czero<V>();
+            line_fft<V, N, -1>(v, tw);
+            V *cb = A + pl * N * PAD + ln;
+#pragma unroll
+            for (int i = 0; i < N; i++) cb[i * PAD] = v[i];
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < N; i++) v[i] = row[i];
+            line_fft<V, N, -1>(v, tw);
+#pragma unroll
+            for (int i = 0; i < N; i++) row[i] = v[i];
+            __syncthreads();
+            if (mine) {
+                V *dstp = op.refwd_grid(item, b0) + (size_t)z * N * N + ln;
+#pragma unroll 4
+                for (int k = 0; k < N; k++) dstp[(size_t)k * N] = A[pl * N * PAD + k * PAD + ln];
             }
         }
     }

@@ -36,7 +36,7 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
                           fast::smem_z_fast<V, N>(Op::NF), op));
     if (do_xyi) {
         const int nref = Op::REFWD ? Op::NB - 1 : 0;
-        if constexpr (Op::GS == 1 && !Op::REFWD) {
+        if constexpr (Op::GS == 1 && !(Op::REGACC && Op::REFWD)) {
             if (!ipair && !c->no_prefetch)
                 return launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (Op::NB + nref) * gb,
                                      fast::k_xyi_pf<T, N, Op>, dim3((np_i + CF::P - 1) / CF::P), dim3(CF::THREADS),

@@ -400,9 +400,11 @@ struct OpTC3A : OpBase<T> {
     static constexpr int NF = 4, NB = 1 + 3 * NX;
     static constexpr bool REFWD = true;
     static constexpr bool ZSPLIT = false;    // one thread per z-line measured faster here
-    // FP32 column sums per output grid over the chunk's sources: b = 0 -> acc,
-    // b = 1 + 3 xs + d -> qsum[d] when xs == s (the other branch only re-forwards)
-    static constexpr bool REGACC = true, BOUTER = true;
+    // accumulation through xyi_accum (FP64 red.add per source), so that the
+    // prefetching XYI kernel can transform the re-forwarded planes in place;
+    // with REGACC the per-output FP32 column sums over the chunk's sources
+    // (b = 0 -> acc, b = 1 + 3 xs + d -> qsum[d] when xs == s) are used instead
+    static constexpr bool REGACC = false, BOUTER = true;
     __device__ bool regacc_grid(int b) const { return b == 0 || EQ || (b - 1) / 3 == s; }
     __device__ V xyi_term(int, int item, int b, size_t p, const V *v) const
     {
