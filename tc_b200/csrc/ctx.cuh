@@ -120,7 +120,7 @@ struct tcg_ctx {
     int ftab_nrec = 1;
     int fast_n = 0;                         // cubic grid size with compiled fast kernels (0: generic path)
     bool force_generic = false;             // use the generic pass kernels even if fast_n is set
-    int xy_kernels = 0;                     // fast XY passes: 0 per-term choice, 1 all line, 2 all lane-pair
+    int xy_kernels = 0;                     // fast XY passes: 0 default, 1 all line, 2 all lane-pair, 3 six threads per line (36^3)
     bool no_prefetch = false;               // fast XYI: no prefetch of the next plane set
     const char *stage = "misc";            // profiling tag of untagged launches (the current stage)
     int z_kernels = 0;                      // fast Z pass: 0 per-term choice, 1 one thread per line, 2 lane pairs

@@ -603,6 +603,191 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2)
     }
 }
 
+// ------------------------------------------ XY passes, 36 = 6 x 6, t6 --
+// For N = 36 each line is transformed by six threads in two radix-6 stages
+// (Cooley-Tukey, 36 = 6 x 6) exchanged through the plane in shared memory:
+// stage 1, thread t: u_t[k1] = w36^{t k1} DFT6_m(x[t + 6 m]);
+// stage 2, thread t as k1: X[k1 + 6 k2] = DFT6_t'(u_t'[k1]).
+// A thread holds 6 values instead of 36, so a CTA of one plane (216
+// threads) needs few registers and many CTAs stay resident.  Thread mapping
+// r = t * 36 + l: consecutive lanes own consecutive lines l, so the row
+// sweeps (stride 37) and the column sweeps (stride 1 across lanes) are free
+// of bank conflicts and the global copies are coalesced along x.
+namespace t6 {
+constexpr int N = 36, R = 6, PAD = 37, THREADS = R * N;
+
+template <typename V>
+struct Tw {
+    const V *w;    // [36] exp(-2 pi i j/36)
+    const V *w6;   // [6]  exp(-2 pi i j/6)
+};
+
+// line element i at base[i * stride]; all threads of the CTA call it.
+// On return v[k2] = X[t + 6 k2]; NAT: also written back in natural order.
+template <typename V, int DIR, bool NAT>
+__device__ __forceinline__ void xform(V *base, int stride, int t, const Tw<V> &tw, V (&v)[R])
+{
+    V u[R];
+#pragma unroll
+    for (int m = 0; m < R; m++) u[m] = base[(t + R * m) * stride];
+    line_fft<V, R, DIR>(u, tw.w6);
+#pragma unroll
+    for (int k1 = 1; k1 < R; k1++) {
+        V w = tw.w[t * k1];
+        if (DIR > 0) w.y = -w.y;
+        u[k1] = cmul(u[k1], w);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k1 = 0; k1 < R; k1++) base[(k1 * R + t) * stride] = u[k1];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < R; j++) v[j] = base[(t * R + j) * stride];
+    line_fft<V, R, DIR>(v, tw.w6);
+    if (NAT) {
+        __syncthreads();
+#pragma unroll
+        for (int k2 = 0; k2 < R; k2++) base[(t + R * k2) * stride] = v[k2];
+        __syncthreads();
+    }
+}
+
+template <typename V>
+__device__ __forceinline__ Tw<V> stage(const GridDesc &g, V *tws)
+{
+    const V *src = twsrc<V>(g);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tws[i] = src[i];
+    __syncthreads();
+    if (threadIdx.x < R) tws[64 + threadIdx.x] = tws[R * threadIdx.x];
+    __syncthreads();
+    return Tw<V>{tws, tws + 64};
+}
+
+// XYF: one (item, z) plane per CTA; pair products -> forward XY FFT -> tmp
+template <typename T, class Op>
+__global__ void __launch_bounds__(THREADS, 4) k_xyf_t6(Op op, int nplanes)
+{
+    using V = typename C2<T>::t;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tws = reinterpret_cast<V *>(smem_raw);
+    V *A = tws + 128;                     // [N][PAD]
+    const Tw<V> tw = stage<V>(op.g, tws);
+    const int t = threadIdx.x / N, l = threadIdx.x % N;
+    const int pid = blockIdx.x;
+    if (pid >= nplanes) return;           // uniform over the CTA
+    const int item = pid / N, z = pid % N;
+    const size_t pz = (size_t)z * N * N;
+    for (int f = 0; f < Op::NF; f++) {
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < R; m++) {
+            const int y = t + R * m;
+            A[y * PAD + l] = op.xyf_load(item, f, l, y, z, pz + (size_t)y * N + l);
+        }
+        __syncthreads();
+        V v[R];
+        xform<V, -1, true>(A + l * PAD, 1, t, tw, v);      // rows
+        xform<V, -1, false>(A + l, PAD, t, tw, v);         // columns: v[k2] at y = t + 6 k2
+        V *dst = op.tmp_grid(item, f) + pz + l;
+#pragma unroll
+        for (int k2 = 0; k2 < R; k2++) dst[(size_t)(t + R * k2) * N] = v[k2];
+    }
+}
+
+// XYI: one (target, z) plane per CTA, looping over the chunk's (source,
+// output) steps; the next step's plane is copied asynchronously into the
+// second set.  GS > 1: the first GS - 1 outputs of a group wait in registers.
+template <typename T, class Op>
+__global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
+{
+    using V = typename C2<T>::t;
+    constexpr int PS = N * PAD;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tws = reinterpret_cast<V *>(smem_raw);
+    V *W = tws + 128;                     // [2][N][PAD]
+    const Tw<V> tw = stage<V>(op.g, tws);
+    const int t = threadIdx.x / N, l = threadIdx.x % N;
+    const int pid = blockIdx.x;
+    if (pid >= nplanes) return;           // uniform over the CTA
+    const int tj = pid / N, z = pid % N;
+    const size_t pz = (size_t)z * N * N;
+    const int ns = op.nsrc(tj);
+    constexpr bool RACC = Op::REGACC && sizeof(V) == 8;
+    static_assert(!(RACC && Op::REFWD), "re-forwarded outputs accumulate through xyi_accum");
+    static_assert(!(Op::REFWD && Op::GS > 1), "re-forward needs GS == 1");
+    V racc[R], keep[Op::GS][R];
+#pragma unroll
+    for (int i = 0; i < R; i++) racc[i] = czero<V>();
+    const int total = ns * Op::NB;        // it = si * NB + b
+    auto issue = [&](int it) {
+        const V *src = op.xyi_grid(op.item_of(tj, it / Op::NB), it % Op::NB) + pz + l;
+        V *dst = W + (it & 1) * PS + l;
+#pragma unroll
+        for (int m = 0; m < R; m++) cp_async_elem(dst + (t + R * m) * PAD, src + (size_t)(t + R * m) * N);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    issue(0);
+    for (int it = 0; it < total; it++) {
+        __syncthreads();                  // the set that step it + 1 overwrites is no longer read
+        if (it + 1 < total) {
+            issue(it + 1);
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        }
+        __syncthreads();
+        const int si = it / Op::NB, b = it % Op::NB, q = b % Op::GS, b0 = b - q;
+        V *A = W + (it & 1) * PS;
+        V v[R];
+        xform<V, +1, true>(A + l * PAD, 1, t, tw, v);      // rows
+        xform<V, +1, false>(A + l, PAD, t, tw, v);         // columns: v[k2] at y = t + 6 k2
+        if (Op::GS > 1 && q < Op::GS - 1) {
+#pragma unroll
+            for (int k2 = 0; k2 < R; k2++) keep[q][k2] = v[k2];
+            continue;
+        }
+        const int item = op.item_of(tj, si);
+        if (RACC && op.regacc_grid(b0)) {
+#pragma unroll
+            for (int k2 = 0; k2 < R; k2++) {
+                V vals[1] = {v[k2]};
+                racc[k2] = cadd(racc[k2], op.xyi_term(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals));
+            }
+        } else {
+#pragma unroll
+            for (int k2 = 0; k2 < R; k2++) {
+                V vals[Op::GS];
+#pragma unroll
+                for (int g = 0; g < Op::GS - 1; g++) vals[g] = keep[g][k2];
+                vals[Op::GS - 1] = v[k2];
+                op.xyi_accum(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals);
+            }
+        }
+        if (Op::REFWD && op.refwd_want(b0)) {   // uniform over the CTA
+            // derived plane (orbital x density) -> forward XY FFT in place -> global
+            __syncthreads();                      // the column sweep has read the set
+#pragma unroll
+            for (int k2 = 0; k2 < R; k2++) {
+                const int y = t + R * k2;
+                A[y * PAD + l] = op.refwd_load(tj, item, b0, pz + (size_t)y * N + l, v[k2]);
+            }
+            __syncthreads();
+            xform<V, -1, true>(A + l, PAD, t, tw, v);      // columns
+            xform<V, -1, true>(A + l * PAD, 1, t, tw, v);  // rows
+            V *dst = op.refwd_grid(item, b0) + pz + l;
+#pragma unroll
+            for (int m = 0; m < R; m++) dst[(size_t)(t + R * m) * N] = A[(t + R * m) * PAD + l];
+        }
+    }
+    if (RACC) {
+#pragma unroll
+        for (int k2 = 0; k2 < R; k2++) op.xyi_flush(tj, pz + (size_t)(t + R * k2) * N + l, racc[k2]);
+    }
+}
+
+template <typename V> __host__ inline size_t smem(int sets) { return sizeof(V) * (128 + (size_t)sets * N * PAD); }
+} // namespace t6
+
 // ------------------------------------------------- XY passes, line pairs --
 // The same XY passes with each row / column split over a lane pair
 // (s = lane & 1, as in the Z pass): half the registers per thread, so twice

@@ -16,7 +16,17 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
     using CP = fast::CfgP<N, sizeof(V)>;
     const bool fpair = c->xy_kernels ? c->xy_kernels == 2 : Op::XYF_PAIR;
     const bool ipair = c->xy_kernels ? c->xy_kernels == 2 : Op::XYI_PAIR;
-    if (do_xyf) {
+    // N = 36: the inverse XY pass runs with six threads per line (t6) unless a
+    // form is forced; the forward pass measured faster with one thread per
+    // line in FP32 and with t6 in FP64 (where a 36-point line spills)
+    const bool t6i = N == 36 && (c->xy_kernels == 0 || c->xy_kernels == 3);
+    const bool t6f = N == 36 && (c->xy_kernels == 3 || (c->xy_kernels == 0 && sizeof(V) == 16));
+    if constexpr (N == 36) {
+        if (t6f && do_xyf)
+            TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * Op::NF * gb, fast::t6::k_xyf_t6<T, Op>,
+                              dim3(np_f), dim3(fast::t6::THREADS), fast::t6::smem<V>(1), op, np_f));
+    }
+    if (do_xyf && !t6f) {
         if (!fpair)
             TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * Op::NF * gb, fast::k_xyf_fast<T, N, Op>,
                               dim3((np_f + CF::P - 1) / CF::P), dim3(CF::THREADS), fast::smem_xy_fast<V, N>(1), op, np_f));
@@ -34,6 +44,14 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
         TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb,
                           fast::k_z_line<T, N, Op>, dim3((N * N + TC - 1) / TC, items), dim3(32 * fast::ZL),
                           fast::smem_z_fast<V, N>(Op::NF), op));
+    if constexpr (N == 36) {
+        if (t6i && do_xyi) {
+            const int nref = Op::REFWD ? Op::NB - 1 : 0;
+            return launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (Op::NB + nref) * gb,
+                                 fast::t6::k_xyi_t6<T, Op>, dim3(np_i), dim3(fast::t6::THREADS), fast::t6::smem<V>(2),
+                                 op, np_i);
+        }
+    }
     if (do_xyi) {
         const int nref = Op::REFWD ? Op::NB - 1 : 0;
         if constexpr (Op::GS == 1 && !(Op::REGACC && Op::REFWD)) {
