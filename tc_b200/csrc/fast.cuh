@@ -785,6 +785,64 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
     }
 }
 
+// Z pass: one item and 32 consecutive pencils (x, y) per CTA, six threads
+// per z-line (warp t owns z = t + 6 m of all 32 pencils).  The NF inputs are
+// transformed in place in S[f][z][32]; each output is combined into O[z][32]
+// and transformed back from there.
+constexpr int ZTHREADS = R * 32;
+template <typename T, class Op>
+__global__ void __launch_bounds__(ZTHREADS, 4) k_z_t6(Op op)
+{
+    using V = typename C2<T>::t;
+    constexpr int TC = 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tws = reinterpret_cast<V *>(smem_raw);
+    V *S = tws + 128;                     // [NF][N][TC]
+    V *O = S + Op::NF * N * TC;           // [N][TC]
+    const Tw<V> tw = stage<V>(op.g, tws);
+    const int item = blockIdx.y;
+    const int t = threadIdx.x / TC, cl = threadIdx.x % TC;
+    const int c = blockIdx.x * TC + cl;
+    const bool act = c < N * N;
+    const int x = c % N, y = c / N;
+#pragma unroll
+    for (int f = 0; f < Op::NF; f++) {
+        const V *src = op.zin_grid(item, f) + c;
+#pragma unroll
+        for (int m = 0; m < R; m++) {
+            const int z = t + R * m;
+            S[(f * N + z) * TC + cl] = act ? src[(size_t)z * N * N] : czero<V>();
+        }
+    }
+    __syncthreads();
+    V v[R];
+#pragma unroll
+    for (int f = 0; f < Op::NF; f++) xform<V, -1, true>(S + f * N * TC + cl, TC, t, tw, v);
+    for (int o = 0; o < Op::NB; o++) {
+        if (Op::ZINV) __syncthreads();    // the previous output's sweep has read O
+#pragma unroll
+        for (int m = 0; m < R; m++) {
+            const int z = t + R * m;
+            V vin[Op::NF];
+#pragma unroll
+            for (int f = 0; f < Op::NF; f++) vin[f] = S[(f * N + z) * TC + cl];
+            const V r = act ? op.zmix(item, o, x, y, z, vin) : czero<V>();
+            if (Op::ZINV) O[z * TC + cl] = r;
+            else if (act) op.out_grid(item, o)[c + (size_t)z * N * N] = r;   // G-space output
+        }
+        if (Op::ZINV) {
+            __syncthreads();
+            xform<V, +1, false>(O + cl, TC, t, tw, v);   // v[k2] at z = t + 6 k2
+            if (act) {
+                V *dst = op.out_grid(item, o) + c;
+#pragma unroll
+                for (int k2 = 0; k2 < R; k2++) dst[(size_t)(t + R * k2) * N * N] = v[k2];
+            }
+        }
+    }
+}
+template <typename V> __host__ inline size_t smem_z(int nf) { return sizeof(V) * (128 + (size_t)(nf + 1) * N * 32); }
+
 template <typename V> __host__ inline size_t smem(int sets) { return sizeof(V) * (128 + (size_t)sets * N * PAD); }
 } // namespace t6
 

@@ -36,7 +36,17 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
     }
     constexpr int TC = fast::zcols<V>();
     const bool zsplit = c->z_kernels ? c->z_kernels == 2 : Op::ZSPLIT;
-    if (zsplit)
+    // N = 36: six threads per z-line unless a form is forced
+    bool zt6 = false;
+    if constexpr (N == 36) {
+        zt6 = c->z_kernels == 0 || c->z_kernels == 3;
+        if (zt6)
+            TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb,
+                              fast::t6::k_z_t6<T, Op>, dim3((N * N + TC - 1) / TC, items), dim3(fast::t6::ZTHREADS),
+                              fast::t6::smem_z<V>(Op::NF), op));
+    }
+    if (zt6) {
+    } else if (zsplit)
         TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb,
                           fast::k_z_fast<T, N, Op>, dim3((N * N + TC - 1) / TC, items), dim3(128),
                           fast::smem_z_fast<V, N>(Op::NF), op));

@@ -177,6 +177,23 @@ def test_36_xy_forms(monkeypatch, method, xy, prec, tol):
         assert rel(g3, r3) < tol
 
 
+@pytest.mark.parametrize("zform", ["line", "split"])
+@pytest.mark.parametrize("method", ["HF", "TC", "BITC"])
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_36_z_forms(monkeypatch, method, zform, prec, tol):
+    """36^3: the Z pass with one thread or a lane pair per z-line (six threads per line is the default there)"""
+    monkeypatch.setenv("TCG_Z_KERNELS", zform)
+    s = system(method, nr=(36, 36, 36), nk=2, ecut=2.0, nbands=2, nocc=1)
+    mask = abi.TERMS_HF if method == "HF" else abi.TERMS_TC
+    r2, r3 = oracle_terms(s, mask)
+    with Context(s, prec) as ctx:
+        ctx.set_state()
+        g2, g3 = ctx.apply(mask)
+    assert rel(g2, r2) < tol
+    if method != "HF":
+        assert rel(g3, r3) < tol
+
+
 @pytest.mark.parametrize("method", ["HF", "BITC"])
 def test_generic_path_noncubic(method):
     """non-cubic grid -> generic (runtime-size) pass kernels"""
