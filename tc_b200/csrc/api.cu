@@ -191,7 +191,7 @@ extern "C" int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg
         c->xy_kernels = !strcmp(e, "line") ? 1 : (!strcmp(e, "pair") ? 2 : (!strcmp(e, "t6") ? 3 : 0));
     if (getenv("TCG_NO_PREFETCH")) c->no_prefetch = true;
     if (const char *e = getenv("TCG_Z_KERNELS"))    // "line" / "split": override the per-term choice
-        c->z_kernels = !strcmp(e, "line") ? 1 : (!strcmp(e, "split") ? 2 : (!strcmp(e, "t6") ? 3 : 0));
+        c->z_kernels = !strcmp(e, "line") ? 1 : (!strcmp(e, "split") ? 2 : (!strcmp(e, "t6") ? 3 : (!strcmp(e, "t6r") ? 4 : 0)));
     *out = c;
     return TCG_OK;
 }

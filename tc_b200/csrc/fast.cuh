@@ -842,6 +842,84 @@ __global__ void __launch_bounds__(ZTHREADS, 4) k_z_t6(Op op)
     }
 }
 template <typename V> __host__ inline size_t smem_z(int nf) { return sizeof(V) * (128 + (size_t)(nf + 1) * N * 32); }
+// Z pass with the transformed inputs kept in registers: thread (t, pencil)
+// runs stage 1 of each input's z-line straight from global memory
+// (z = t + 6 m), exchanges once through shared memory, and after stage 2
+// holds every input at z = t + 6 k2 -- the points where it evaluates the
+// G-space combination of every output.  Those values are already in the
+// input order of the inverse transform's stage 1, so each output needs one
+// exchange only.  Shared memory: one exchange buffer per input.
+template <typename T, class Op>
+__global__ void __launch_bounds__(ZTHREADS, 3) k_z_t6r(Op op)
+{
+    using V = typename C2<T>::t;
+    constexpr int TC = 32, NF = Op::NF;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tws = reinterpret_cast<V *>(smem_raw);
+    V *E = tws + 128;                     // [NF][N][TC] exchange buffers
+    const Tw<V> tw = stage<V>(op.g, tws);
+    const int item = blockIdx.y;
+    const int t = threadIdx.x / TC, cl = threadIdx.x % TC;
+    const int c = blockIdx.x * TC + cl;
+    const bool act = c < N * N;
+    const int x = c % N, y = c / N;
+    V X[NF][R];
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+        const V *src = op.zin_grid(item, f) + c;
+#pragma unroll
+        for (int m = 0; m < R; m++) X[f][m] = act ? src[(size_t)(t + R * m) * N * N] : czero<V>();
+    }
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+        line_fft<V, R, -1>(X[f], tw.w6);
+#pragma unroll
+        for (int k1 = 0; k1 < R; k1++) {
+            V u = X[f][k1];
+            if (k1 > 0) u = cmul(u, tw.w[t * k1]);
+            E[(f * N + k1 * R + t) * TC + cl] = u;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+#pragma unroll
+        for (int j = 0; j < R; j++) X[f][j] = E[(f * N + t * R + j) * TC + cl];
+        line_fft<V, R, -1>(X[f], tw.w6);   // X[f][k2]: input f at z = t + 6 k2
+    }
+    for (int o = 0; o < Op::NB; o++) {
+        V v[R];
+#pragma unroll
+        for (int k2 = 0; k2 < R; k2++) {
+            V vin[NF];
+#pragma unroll
+            for (int f = 0; f < NF; f++) vin[f] = X[f][k2];
+            v[k2] = act ? op.zmix(item, o, x, y, t + R * k2, vin) : czero<V>();
+        }
+        if (Op::ZINV) {
+            // inverse: stage 1 over m = k2 in registers, one exchange, stage 2
+            line_fft<V, R, +1>(v, tw.w6);
+            __syncthreads();                  // the exchange buffer is free
+#pragma unroll
+            for (int k1 = 0; k1 < R; k1++) {
+                V u = v[k1];
+                if (k1 > 0) { V w = tw.w[t * k1]; w.y = -w.y; u = cmul(u, w); }
+                E[(k1 * R + t) * TC + cl] = u;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < R; j++) v[j] = E[(t * R + j) * TC + cl];
+            line_fft<V, R, +1>(v, tw.w6);     // v[k2] at z = t + 6 k2
+        }
+        if (act) {
+            V *dst = op.out_grid(item, o) + c;
+#pragma unroll
+            for (int k2 = 0; k2 < R; k2++) dst[(size_t)(t + R * k2) * N * N] = v[k2];
+        }
+    }
+}
+template <typename V> __host__ inline size_t smem_zr(int nf) { return sizeof(V) * (128 + (size_t)nf * N * 32); }
+
 
 template <typename V> __host__ inline size_t smem(int sets) { return sizeof(V) * (128 + (size_t)sets * N * PAD); }
 } // namespace t6

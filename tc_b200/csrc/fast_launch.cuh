@@ -39,11 +39,17 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
     // N = 36: six threads per z-line unless a form is forced
     bool zt6 = false;
     if constexpr (N == 36) {
-        zt6 = c->z_kernels == 0 || c->z_kernels == 3;
-        if (zt6)
+        zt6 = c->z_kernels == 0 || c->z_kernels == 3 || c->z_kernels == 4;
+        // default: inputs transformed in place in shared memory (k_z_t6); the
+        // terms with Op::ZREG keep them in registers in FP32 (k_z_t6r)
+        if (c->z_kernels == 3 || (c->z_kernels == 0 && !(Op::ZREG && sizeof(V) == 8)))
             TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb,
                               fast::t6::k_z_t6<T, Op>, dim3((N * N + TC - 1) / TC, items), dim3(fast::t6::ZTHREADS),
                               fast::t6::smem_z<V>(Op::NF), op));
+        else if (zt6)
+            TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb,
+                              fast::t6::k_z_t6r<T, Op>, dim3((N * N + TC - 1) / TC, items), dim3(fast::t6::ZTHREADS),
+                              fast::t6::smem_zr<V>(Op::NF), op));
     }
     if (zt6) {
     } else if (zsplit)

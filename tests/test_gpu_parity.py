@@ -177,11 +177,12 @@ def test_36_xy_forms(monkeypatch, method, xy, prec, tol):
         assert rel(g3, r3) < tol
 
 
-@pytest.mark.parametrize("zform", ["line", "split"])
+@pytest.mark.parametrize("zform", ["line", "split", "t6", "t6r"])
 @pytest.mark.parametrize("method", ["HF", "TC", "BITC"])
 @pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
 def test_36_z_forms(monkeypatch, method, zform, prec, tol):
-    """36^3: the Z pass with one thread or a lane pair per z-line (six threads per line is the default there)"""
+    """36^3: every Z pass form (one thread, a lane pair, six threads per z-line with the inputs in shared
+    memory or in registers)"""
     monkeypatch.setenv("TCG_Z_KERNELS", zform)
     s = system(method, nr=(36, 36, 36), nk=2, ecut=2.0, nbands=2, nocc=1)
     mask = abi.TERMS_HF if method == "HF" else abi.TERMS_TC
