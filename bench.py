@@ -413,7 +413,8 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": "BITC batched apply, same as the GPU arm", "config": args.config},
+            "config": {"workload": WORKLOADS.get(args.config, args.config), "config": args.config,
+                       "band_applies_per_step": int(system.nb_apply.sum()), "parallelism": "host threads"},
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

@@ -158,10 +158,11 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 3)
     const int pid0 = blockIdx.x * P;
     for (int f = 0; f < Op::NF; f++) {
         __syncthreads();
-        // each thread fills column x = ln of its own plane (item and z fixed)
+        // each thread fills column x = ln of its own plane (item and z fixed);
+        // 12 elements (24 loads) in flight per thread
         if (pid0 + pl < nplanes) {
             const int item = (pid0 + pl) / N, z = (pid0 + pl) % N;
-#pragma unroll 4
+#pragma unroll 12
             for (int k = 0; k < N; k++)
                 A[pl * N * PAD + k * PAD + ln] = op.xyf_load(item, f, ln, k, z, (size_t)z * N * N + (size_t)k * N + ln);
         }
