@@ -115,15 +115,9 @@ def dist_info():
 
 
 def shard_owned(system, world, rank):
-    """Band-applies sharded over ranks by k-point, round robin
-    (Parallelization::set_orbital_parallelization splits (spin, k, band)
-    blocks, parallelization.cpp:127-172)."""
-    flags = []
-    for s in range(system.nspin):
-        for k in range(system.nk_irr):
-            own = (k % world) == rank
-            flags += [1 if own else 0] * int(system.nb_apply[s][k])
-    return np.array(flags, dtype=np.uint8)
+    """Band-applies sharded over ranks by k-point (tc_b200.sharding.owned_mask)."""
+    from tc_b200.sharding import owned_mask
+    return owned_mask(system, world, rank)
 
 
 # ---------------------------------------------------------- FFT model ---
@@ -146,6 +140,7 @@ def run_ours(args):
     import torch.distributed as dist
     from tc_b200 import abi, synth
     from tc_b200.context import Context
+    from tc_b200.sharding import sharded_qp_stage
 
     world, rank, local = dist_info()
     torch.cuda.set_device(local)
@@ -179,11 +174,16 @@ def run_ours(args):
         h3 = torch.zeros(n2, dtype=torch.float64, device=dev)
         stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
 
+        def state():
+            ctx.refresh_state()
+            if world > 1 and mask & abi.TERM_TC3A2A4B2B5:
+                sharded_qp_stage(ctx)       # (q1, i1) split + NCCL all_reduce of the partial grids
+
         def step():
             h2.zero_()
             h3.zero_()
             torch.cuda.synchronize()
-            ctx.refresh_state()
+            state()
             ctx.apply_device(mask, psi_dev.data_ptr(), h2.data_ptr(), h3.data_ptr(), owned=owned)
 
         for _ in range(warmup):
@@ -204,7 +204,7 @@ def run_ours(args):
             e1 = torch.cuda.Event(enable_timing=True)
             torch.cuda.nvtx.range_push("bench_timed")   # ncu --nvtx-include "bench_timed]"
             e0.record(stream)
-            ctx.refresh_state()
+            state()
             ctx.apply_device(mask, psi_dev.data_ptr(), h2.data_ptr(), h3.data_ptr(), owned=owned)
             e1.record(stream)
             torch.cuda.nvtx.range_pop()
@@ -229,7 +229,7 @@ def run_ours(args):
     t_mixed = max_over_ranks(sum(mixed["times"]))
     fp64 = None
     if not args.no_fp64:
-        fp64 = device_arm("fp64", max(1, args.fp64_steps), 1)
+        fp64 = device_arm("fp64", args.fp64_steps or args.steps, args.warmup)
         t_fp64 = max_over_ranks(sum(fp64["times"]))
 
     # ---- end to end through the C-ABI with pinned host buffers
@@ -280,12 +280,15 @@ def run_ours(args):
             dist.destroy_process_group()
         return
 
-    # ---- energies and |dE| (mixed vs FP64)
+    # ---- energies and |dE| (mixed vs the FP64 oracle, and vs the GPU's FP64 form)
     e_mixed = system.energy_terms(mixed["h2"], mixed["h3"])
     dE = None
     if fp64 is not None:
         e_fp64 = system.energy_terms(fp64["h2"], fp64["h3"])
         dE = abs(sum(e_mixed) - sum(e_fp64))
+    e_oracle = oracle_energy(args.config)
+    dE_oracle = None if e_oracle is None else abs(sum(e_mixed) - e_oracle)
+    dE_fp64_oracle = None if (e_oracle is None or fp64 is None) else abs(sum(e_fp64) - e_oracle)
     value = nb_total * args.steps / t_mixed
     pk, pk_kind = peaks()
     # ---- roofline of the dominant kernel (pass tag with the most device time)
@@ -322,6 +325,8 @@ def run_ours(args):
                                            "ms_per_step": round(t_fp64 / len(fp64["times"]) * 1e3, 2)},
         "mixed_over_fp64": None if fp64 is None else round((nb_total * args.steps / t_mixed) /
                                                            (nb_total * len(fp64["times"]) / t_fp64), 3),
+        "dE_mixed_vs_oracle_Ha": dE_oracle,
+        "dE_fp64_vs_oracle_Ha": dE_fp64_oracle,
         "dE_mixed_vs_fp64_Ha": dE,
         "energy": {"E2": [e_mixed[0].real, e_mixed[0].imag], "E3": [e_mixed[1].real, e_mixed[1].imag]},
         "roofline": roof,
@@ -338,6 +343,18 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def oracle_energy(config):
+    """E2 + E3 of the occupied orbitals from the FP64 CPU oracle, committed
+    with the workload's parity fixture (tests/golden/make_c3_subset.py)."""
+    if config != "C3":
+        return None
+    p = os.path.join(ROOT, "tests", "golden", "c3_subset.npz")
+    if not os.path.exists(p):
+        return None
+    z = np.load(p)
+    return complex(z["E2"]) + complex(z["E3"])
 
 
 def traffic_for(config, tag):
@@ -426,7 +443,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="C3")
-    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--fp64-steps", type=int, default=0, help="0: as many as --steps")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

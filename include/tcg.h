@@ -14,7 +14,7 @@
  * std::vector<...<Eigen::VectorXcd>> containers; here every container is a
  * flat, packed array of interleaved (re, im) doubles -- the memory layout of
  * std::complex<double> / Eigen::VectorXcd -- so the reference's C++ host can
- * pass its buffers after one memcpy per band (see INTEGRATION.md).
+ * pass its buffers after one memcpy per band.
  *
  * Conventions (all follow TC++):
  *  - FFT grid nr[0] x nr[1] x nr[2], x = nr[0] fastest; grid index
@@ -165,6 +165,19 @@ int tcg_apply_device(tcg_ctx *ctx, uint32_t term_mask, const int32_t *nb_apply,
                      const void *psi_dev, void *h2_dev, void *h3_dev,
                      const uint8_t *owned);
 
+/* Two- and three-body energies of the applied bands, reduced on the device in
+ * FP64 (TotalEnergy::calc_total_energy, total_energy.cpp:101-168):
+ *   E_n = sum_{s, k, isym, b} f_b e_n(b) / (n N_k),  n = 2, 3,
+ *   e_n(b) = <chi_kb | h_n b>  (conjugated for time-reversed images),
+ * where chi_kb is band b of the current state's left (BITC) or right
+ * orbitals and h2_dev / h3_dev are DEVICE arrays in the packed layout of
+ * tcg_apply with nb_apply bands per (spin, k) -- e.g. the outputs of
+ * tcg_apply_device with psi = the occupied orbitals.  Either may be NULL
+ * (that energy is then 0).  Bands b >= nbands or with zero filling are
+ * skipped.  e_out[4] = {Re E2, Im E2, Re E3, Im E3} (host).  The sum runs in a
+ * fixed order: repeated calls give identical bits. */
+int tcg_energy(tcg_ctx *ctx, const int32_t *nb_apply, const void *h2_dev, const void *h3_dev, double *e_out);
+
 /* Divergence-correction scalars for the SCF mesh (Potentials::set_sum_of_Vaux
  * with set_sum_of_Vaux_each, potentials_coulomb.cpp:60-161), computed on the
  * device.  Writes alpha_Vaux and sum_Vaux[nk_irr]; needs only the geometry
@@ -172,20 +185,24 @@ int tcg_apply_device(tcg_ctx *ctx, uint32_t term_mask, const int32_t *nb_apply,
 int tcg_sum_of_vaux(const tcg_system_desc *sys, double *alpha_out, double *sum_vaux_out);
 
 /* Allocation-free variant of tcg_sum_of_vaux for callers that cannot
- * allocate device memory -- e.g. code running inside a stream capture or
- * under an external memory pool that forbids cudaMalloc / cudaFree.  No
- * counterpart in the reference (TC++ computes these sums on the host).
+ * allocate device memory: an application or framework whose memory pool has
+ * reserved the GPU's memory up front (a cudaMalloc would fail or fragment the
+ * pool), or code that must not trigger the implicit device-wide
+ * synchronisation of cudaMalloc / cudaFree.  No counterpart in the reference
+ * (TC++ computes these sums on the host).
  * All arrays are DEVICE pointers: kirr_dev [nk_irr][3] and kall_dev
  * [nk_all][3] fractional k-vectors (irreducible k, full SCF mesh), output
  * sum_vaux_dev [nk_irr]; alpha_out is a host pointer (may be NULL).  The
- * work is queued on `stream` (cudaStream_t as void*, NULL = default) and the
- * call returns after it finished.  Scratch is a static device array of
- * 16384 (k, q) pairs held by every GPU that loads the library; larger
- * nk_irr * nk_all is rejected with TCG_ERR_ARG.  The first call on a device
- * looks the array's device address up (cudaGetSymbolAddress) and should
- * come before any stream capture.  Every call shares the one array: calls
- * that overlap on the GPU (other threads or streams) race and must be
- * serialised by the caller. */
+ * work is queued on `stream` (cudaStream_t as void*, NULL = default); the
+ * call then copies a convergence flag to the host and synchronises that
+ * stream before it returns.  Scratch is a static device array of 16384
+ * (k, q) pairs held by every GPU that loads the library until the process
+ * exits; larger nk_irr * nk_all is rejected with TCG_ERR_ARG.  The first call
+ * on a device looks the array's device address up (cudaGetSymbolAddress)
+ * and keeps it for the life of the process: after a cudaDeviceReset of that
+ * device the kept address is stale and the entry point must not be called
+ * again.  Every call shares the one array: calls that overlap on the GPU
+ * (other threads or streams) race and must be serialised by the caller. */
 int tcg_sum_of_vaux_noalloc(const double recip[9], double omega, int32_t nk_irr, int32_t nk_all,
                             const double *kirr_dev, const double *kall_dev, double *sum_vaux_dev,
                             double *alpha_out, void *stream);
@@ -195,6 +212,24 @@ int tcg_sum_of_vaux_noalloc(const double recip[9], double omega, int32_t nk_irr,
  * density_out is [2][N] complex.  Fails with TCG_ERR_NUMERIC if an orbital's
  * norm <chi|phi> deviates from 1 by more than 1e-4 (as the reference). */
 int tcg_density(tcg_ctx *ctx, const tcg_state_desc *st, double *density_out);
+
+/* Occupied-pair stage of tc3a2a4b2b5 split over ranks.  The stage sums, for
+ * every occupied target (q2, i2), intermediates over all occupied sources
+ * (q1, i1); the reference splits the q1 bands over MPI ranks and
+ * MPI_Allreduces the intermediate grids (calc_hamiltonian_tc3a2a4b2b5.cpp:
+ * 214-235, 490-493, 649-659).  Here:
+ *   tcg_qp_partial: this rank's share (the sources in nranks contiguous
+ *     blocks, block `rank`) into a device buffer of FP64 complex grids;
+ *     returns its address and size in bytes.  The caller sums the buffer
+ *     over all ranks in place (e.g. ncclAllReduce of bytes/8 doubles, sum)
+ *     and synchronises, then calls
+ *   tcg_qp_finish: divergence correction, symmetry rotations and the local
+ *     potentials on the summed grids; the next tcg_apply uses the result.
+ * Every rank must call both with the same state.  Without these calls,
+ * tcg_apply computes the whole stage on one rank.  Between the two calls
+ * tcg_apply with the tc3a2a4b2b5 bit fails with TCG_ERR_STATE. */
+int tcg_qp_partial(tcg_ctx *ctx, int32_t rank, int32_t nranks, void **buf_dev, size_t *bytes);
+int tcg_qp_finish(tcg_ctx *ctx);
 
 /* Tuning knob: bytes of pass temporaries one chunk of (target x source)
  * pairs may use (0 = default, 8 GiB).  Smaller chunks keep the temporaries

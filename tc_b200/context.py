@@ -129,6 +129,28 @@ class Context:
                               None if own is None else own.ctypes.data))
         return h2, h3
 
+    def qp_partial(self, rank, nranks):
+        """This rank's share of the tc3a2a4b2b5 occupied-pair stage: returns
+        (device pointer, bytes) of the FP64 buffer the caller must sum over
+        ranks before qp_finish()."""
+        p = C.c_void_p()
+        n = C.c_size_t()
+        check(lib().tcg_qp_partial(self.handle, int(rank), int(nranks), C.byref(p), C.byref(n)))
+        return int(p.value or 0), int(n.value)
+
+    def qp_finish(self):
+        check(lib().tcg_qp_finish(self.handle))
+
+    def energy_device(self, h2_ptr, h3_ptr, nb_apply=None):
+        """(E2, E3) of the applied bands from DEVICE arrays h2 / h3 (packed like
+        psi; pointers as ints, 0 = skip), reduced on the GPU in FP64."""
+        s = self.system
+        nb = np.ascontiguousarray(s.nb_apply if nb_apply is None else nb_apply, dtype=np.int32)
+        out = (C.c_double * 4)()
+        check(lib().tcg_energy(self.handle, nb.ctypes.data_as(C.POINTER(C.c_int32)), C.c_void_p(h2_ptr or None),
+                               C.c_void_p(h3_ptr or None), out))
+        return complex(out[0], out[1]), complex(out[2], out[3])
+
     def apply_device(self, terms, psi_ptr, h2_ptr, h3_ptr, nb_apply=None, owned=None):
         """Device-memory apply on the context's stream (pointers as ints)."""
         s = self.system

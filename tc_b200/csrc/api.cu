@@ -190,6 +190,7 @@ extern "C" int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg
     if (const char *e = getenv("TCG_XY_KERNELS"))   // "line" / "pair": override the per-term choice
         c->xy_kernels = !strcmp(e, "line") ? 1 : (!strcmp(e, "pair") ? 2 : (!strcmp(e, "t6") ? 3 : 0));
     if (getenv("TCG_NO_PREFETCH")) c->no_prefetch = true;
+    if (const char *e = getenv("TCG_MIN_TARGETS")) c->min_targets = atoi(e);
     if (const char *e = getenv("TCG_Z_KERNELS"))    // "line" / "split": override the per-term choice
         c->z_kernels = !strcmp(e, "line") ? 1 : (!strcmp(e, "split") ? 2 : (!strcmp(e, "t6") ? 3 : (!strcmp(e, "t6r") ? 4 : 0)));
     *out = c;
@@ -363,6 +364,32 @@ extern "C" int tcg_apply(tcg_ctx *c, uint32_t mask, const int32_t *nb, const dou
     if (need3) TCG_CUDA(cudaMemcpyAsync(h3, c->h3.p, bytes, cudaMemcpyDeviceToHost, c->stream));
     TCG_CUDA(cudaStreamSynchronize(c->stream));
     return TCG_OK;
+}
+
+extern "C" int tcg_qp_partial(tcg_ctx *c, int32_t rank, int32_t nranks, void **buf_dev, size_t *bytes)
+{
+    if (!c || !buf_dev || !bytes) return fail(TCG_ERR_ARG, "null argument");
+    if (nranks < 1 || rank < 0 || rank >= nranks) return fail(TCG_ERR_ARG, "rank outside [0, nranks)");
+    Host &h = c->h;
+    if (!h.have_state) return fail(TCG_ERR_STATE, "tcg_set_state must be called before tcg_qp_partial");
+    if (h.method == TCG_METHOD_HF) return fail(TCG_ERR_ARG, "HF contexts have no tc3a2a4b2b5 stage");
+    h.qp_ready = false;
+    h.qp_pending = false;
+    TRY(c->prec == TCG_PREC_FP64 ? qp_partial<double>(c, rank, nranks) : qp_partial<float>(c, rank, nranks));
+    const std::vector<size_t> off = qp_acc_offsets(c);
+    *buf_dev = c->accP.p;
+    *bytes = off[h.nspin] * (size_t)h.N * sizeof(double2);
+    h.qp_pending = true;
+    return TCG_OK;
+}
+
+extern "C" int tcg_qp_finish(tcg_ctx *c)
+{
+    if (!c) return fail(TCG_ERR_ARG, "null context");
+    Host &h = c->h;
+    if (!h.qp_pending) return fail(TCG_ERR_STATE, "tcg_qp_finish without a pending tcg_qp_partial");
+    h.qp_pending = false;
+    return c->prec == TCG_PREC_FP64 ? qp_finish<double>(c) : qp_finish<float>(c);
 }
 
 extern "C" int tcg_set_tuning(tcg_ctx *c, int64_t tmp_budget_bytes)
@@ -571,6 +598,105 @@ extern "C" int tcg_density(tcg_ctx *c, const tcg_state_desc *st, double *out)
         const double re = n.x / (double)N - 1.0, im = n.y / (double)N;
         if (std::sqrt(re * re + im * im) > 1e-4) return fail(TCG_ERR_NUMERIC, "normalization breaks");
     }
+    return TCG_OK;
+}
+
+// ------------------------------------------------------------ energies --
+// e_n of one applied band: <chi_b | h_n b> over its plane waves (fixed-order
+// tree reduction), one block per (spin, k, band) with a non-zero filling.
+struct EnergyBand {
+    const double2 *bra;      // left (BITC) or right orbital of the band, G space
+    const double2 *h2, *h3;  // applied terms of the band (nullptr: skipped)
+    int npw;
+};
+static __global__ void __launch_bounds__(256) k_band_dots(const EnergyBand *bands, double2 *dots)
+{
+    const EnergyBand b = bands[blockIdx.x];
+    __shared__ double2 red[2][256];
+    double2 a2 = {0, 0}, a3 = {0, 0};
+    for (int p = threadIdx.x; p < b.npw; p += blockDim.x) {
+        const double2 c = b.bra[p];
+        if (b.h2) a2 = cadd(a2, cmulc(c, b.h2[p]));
+        if (b.h3) a3 = cadd(a3, cmulc(c, b.h3[p]));
+    }
+    red[0][threadIdx.x] = a2;
+    red[1][threadIdx.x] = a3;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            red[0][threadIdx.x] = cadd(red[0][threadIdx.x], red[0][threadIdx.x + s]);
+            red[1][threadIdx.x] = cadd(red[1][threadIdx.x], red[1][threadIdx.x + s]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        dots[2 * blockIdx.x] = red[0][0];
+        dots[2 * blockIdx.x + 1] = red[1][0];
+    }
+}
+// E_n = sum_bands f (n_plain e_n + n_tr conj(e_n)) / (n N_k): one thread,
+// bands in order, so the sum is reproducible bit for bit
+static __global__ void k_energy_sum(int nband, const double2 *dots, const double *w, double inv_nk, double *out)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double2 e2 = {0, 0}, e3 = {0, 0};
+    for (int i = 0; i < nband; i++) {
+        const double wp = w[2 * i], wt = w[2 * i + 1];   // f * (images without / with time reversal)
+        const double2 d2 = dots[2 * i], d3 = dots[2 * i + 1];
+        e2.x += (wp + wt) * d2.x; e2.y += (wp - wt) * d2.y;
+        e3.x += (wp + wt) * d3.x; e3.y += (wp - wt) * d3.y;
+    }
+    out[0] = e2.x * inv_nk / 2.0; out[1] = e2.y * inv_nk / 2.0;
+    out[2] = e3.x * inv_nk / 3.0; out[3] = e3.y * inv_nk / 3.0;
+}
+
+extern "C" int tcg_energy(tcg_ctx *c, const int32_t *nb, const void *h2_dev, const void *h3_dev, double *e_out)
+{
+    if (!c || !nb || !e_out) return fail(TCG_ERR_ARG, "null argument");
+    Host &h = c->h;
+    if (!h.have_state) return fail(TCG_ERR_STATE, "tcg_set_state must be called before tcg_energy");
+    const bool bitc = h.method == TCG_METHOD_BITC;
+    std::vector<EnergyBand> bands;
+    std::vector<double> w;
+    size_t off = 0;
+    for (int s = 0; s < h.nspin; s++)
+        for (int k = 0; k < h.nk; k++) {
+            if (nb[s * h.nk + k] < 0) return fail(TCG_ERR_ARG, "negative band count");
+            int nplain = 0, ntr = 0;
+            for (int a = h.kall_off[k]; a < h.kall_off[k + 1]; a++) (h.time_rev[a] ? ntr : nplain)++;
+            for (int b = 0; b < nb[s * h.nk + k]; b++, off += h.npw[k]) {
+                if (b >= h.nbands[s]) continue;
+                const double f = h.filling[fill_off(h, s, k) + b];
+                if (f == 0.0) continue;
+                EnergyBand e;
+                e.bra = (bitc ? c->chik.as<double2>() : c->phik.as<double2>()) + h.orb_off[(size_t)s * h.nk + k] +
+                        (size_t)b * h.npw[k];
+                e.h2 = h2_dev ? (const double2 *)h2_dev + off : nullptr;
+                e.h3 = h3_dev ? (const double2 *)h3_dev + off : nullptr;
+                e.npw = h.npw[k];
+                bands.push_back(e);
+                w.push_back(f * nplain);
+                w.push_back(f * ntr);
+            }
+        }
+    if (bands.empty()) {
+        for (int i = 0; i < 4; i++) e_out[i] = 0.0;
+        return TCG_OK;
+    }
+    const size_t nbd = bands.size();
+    DBuf &buf = c->aux;
+    const size_t b0 = 0, b1 = (nbd * sizeof(EnergyBand) + 255) & ~(size_t)255;
+    const size_t b2 = b1 + ((nbd * 2 * sizeof(double) + 255) & ~(size_t)255);
+    const size_t b3 = b2 + ((nbd * 2 * sizeof(double2) + 255) & ~(size_t)255);
+    TRY(buf.ensure(b3 + 4 * sizeof(double)));
+    char *base = buf.as<char>();
+    TCG_CUDA(cudaMemcpyAsync(base + b0, bands.data(), nbd * sizeof(EnergyBand), cudaMemcpyHostToDevice, c->stream));
+    TCG_CUDA(cudaMemcpyAsync(base + b1, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    TRY(launch(c, k_band_dots, dim3((unsigned)nbd), dim3(256), 0, (const EnergyBand *)(base + b0), (double2 *)(base + b2)));
+    TRY(launch(c, k_energy_sum, dim3(1), dim3(1), 0, (int)nbd, (const double2 *)(base + b2), (const double *)(base + b1),
+               1.0 / h.num_kpoints, (double *)(base + b3)));
+    TCG_CUDA(cudaMemcpyAsync(e_out, base + b3, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    TCG_CUDA(cudaStreamSynchronize(c->stream));
     return TCG_OK;
 }
 

@@ -82,6 +82,7 @@ struct Host {
     std::vector<size_t> occ_off;            // [nspin*nk_all] grid offset into Rocc
     size_t nocc_grids = 0;
     bool qp_ready = false;                  // tc3a2a4b2b5 occupied-pair stage done for this state
+    bool qp_pending = false;                // a partial stage awaits the caller's sum and tcg_qp_finish
 };
 
 struct tcg_ctx_impl;
@@ -124,7 +125,8 @@ struct tcg_ctx {
     bool no_prefetch = false;               // fast XYI: no prefetch of the next plane set
     const char *stage = "misc";            // profiling tag of untagged launches (the current stage)
     int z_kernels = 0;                      // fast Z pass: 0 per-term choice, 1 one thread per line, 2 lane pairs
-    size_t tmp_budget = 0;                  // bytes per chunk of pass temporaries (0: default 1 GiB)
+    size_t tmp_budget = 0;                  // bytes per chunk of pass temporaries (0: default 8 GiB)
+    int min_targets = 0;                    // targets per chunk (0: default, about 12 waves of XYI CTAs)
     int64_t launches = 0;
     // optional per-kernel timing with CUDA events on the context stream
     bool prof = false;

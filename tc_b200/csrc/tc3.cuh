@@ -412,9 +412,11 @@ static int plan_chunks(tcg_ctx *c, DBuf &meta, int ntg, const std::vector<int> &
 }
 
 // targets per chunk: the XYI pass runs one CTA per (target, plane group)
-// and loops over the chunk's sources, so give it ~12 waves of CTAs
+// and loops over the chunk's sources.  c->min_targets > 0 (TCG_MIN_TARGETS)
+// overrides the default of ~12 waves of CTAs.
 static int min_targets(const tcg_ctx *c)
 {
+    if (c->min_targets > 0) return c->min_targets;
     const int n2 = c->h.n[2];
     return std::max(1, (148 * 3 * 12 * 4 + n2 - 1) / n2);
 }
@@ -855,16 +857,21 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
     return TCG_OK;
 }
 
-// occupied-pair chunks of tc3a2a4b2b5 for spin sq
+// occupied-pair chunks of tc3a2a4b2b5 for spin sq, sources [lo, hi) of S
 template <typename T, bool BITC, bool EQ>
 static int qp_pairs(tcg_ctx *c, int sq, int ntq, const std::vector<int> &tkey, const std::vector<double> &tcart,
-                    const Sources &S, double2 *accP, int nacc)
+                    const Sources &S0, int lo, int hi, double2 *accP, int nacc)
 {
     using V = typename C2<T>::t;
     using OQ = OpQP<T, BITC, EQ>;
     const Host &h = c->h;
     const size_t N = h.N;
     const int nsl = OQ::NB;
+    if (hi <= lo) return TCG_OK;
+    Sources S;
+    S.base = S0.base + lo;
+    S.key.assign(S0.key.begin() + lo, S0.key.begin() + hi);
+    S.cartq.assign(S0.cartq.begin() + 3 * (size_t)lo, S0.cartq.begin() + 3 * (size_t)hi);
     std::vector<ChunkPlan> plan;
     TRY(plan_chunks(c, c->meta, ntq, tkey, tcart, (int)S.key.size(), S.key, S.cartq, max_items_for(c, nsl, sizeof(V)),
                     min_targets(c), plan));
@@ -889,8 +896,95 @@ static int qp_pairs(tcg_ctx *c, int sq, int ntq, const std::vector<int> &tkey, c
 }
 
 // ------------------------------------ tc3a2a4b2b5: per-state occupied stage --
+// Targets of spin sq: (iq2 irreducible, i2), with their grid index in Rocc.
+struct QPTargets {
+    std::vector<int> key, grid;
+    std::vector<double> cart;
+};
+static QPTargets qp_targets(const tcg_ctx *c, int sq)
+{
+    const Host &h = c->h;
+    QPTargets Q;
+    for (int iq2 = 0; iq2 < h.nk; iq2++) {
+        double q[3];
+        cart(h, &h.kvec[3 * h.kall_off[iq2]], q);
+        for (int i = 0; i < h.nocc[sq * h.nk + iq2]; i++) {
+            Q.key.push_back(iq2);
+            Q.grid.push_back((int)(h.occ_off[(size_t)sq * h.nk_all + h.kall_off[iq2]] + i));
+            Q.cart.insert(Q.cart.end(), q, q + 3);
+        }
+    }
+    return Q;
+}
+
+// Offsets (in grids of N points) of each spin's accumulators in accP:
+// [sq][target][nacc][N], nacc = nspin + 6 (3a2 per spin, 3a4 x3, 3b5 x3).
+static std::vector<size_t> qp_acc_offsets(const tcg_ctx *c)
+{
+    const Host &h = c->h;
+    const int nacc = h.nspin + 6;
+    std::vector<size_t> off(h.nspin + 1, 0);
+    for (int sq = 0; sq < h.nspin; sq++) {
+        size_t ntq = 0;
+        for (int iq2 = 0; iq2 < h.nk; iq2++) ntq += h.nocc[sq * h.nk + iq2];
+        off[sq + 1] = off[sq] + ntq * nacc;
+    }
+    return off;
+}
+
+// First half of the occupied-pair stage (tc3a2a4b2b5.cpp:210-443): the sums
+// over the occupied sources (q1, i1) of the intermediates of every target
+// (q2, i2), accumulated in c->accP.  Sources are split into nranks contiguous
+// blocks and only block `rank` is summed, so that the ranks' partial buffers
+// add up to the whole stage (the reference splits the q1 bands over MPI ranks
+// and MPI_Allreduces these grids, :214-235, :490-493, :649-659).
 template <typename T>
-static int qp_stage(tcg_ctx *c)
+static int qp_partial(tcg_ctx *c, int rank, int nranks)
+{
+    PhaseScope ps_(c, "st:qp");
+    Host &h = c->h;
+    const size_t N = h.N;
+    const int ns = h.nspin;
+    const bool bitc = h.method == TCG_METHOD_BITC;
+    const int nacc = ns + 6;
+    const std::vector<size_t> aoff = qp_acc_offsets(c);
+    TRY(c->accP.ensure(std::max<size_t>(1, aoff[ns]) * N * sizeof(double2)));
+    TRY(launch(c, k_zero, dim3(148 * 8), dim3(256), 0, c->accP.as<double2>(), aoff[ns] * N));
+    using V = typename C2<T>::t;
+    for (int sq = 0; sq < ns; sq++) {
+        const QPTargets Q = qp_targets(c, sq);
+        const int ntq = (int)Q.key.size();
+        if (ntq == 0) continue;
+        Sources S = sources_of(c, sq);
+        const int nsrc = (int)S.key.size();
+        const int lo = (int)((int64_t)nsrc * rank / nranks), hi = (int)((int64_t)nsrc * (rank + 1) / nranks);
+        // target grids are not contiguous in Rocc (isym > 0 grids in between):
+        // gather them into a contiguous copy
+        TRY(c->qtg.ensure((size_t)ntq * 2 * N * sizeof(V)));
+        for (int i = 0; i < ntq; i++) {
+            TCG_CUDA(cudaMemcpyAsync(c->qtg.as<V>() + (size_t)i * N, c->Rocc.as<V>() + (size_t)Q.grid[i] * N,
+                                     N * sizeof(V), cudaMemcpyDeviceToDevice, c->stream));
+            const V *chsrc = bitc ? c->Rchi.as<V>() : c->Rocc.as<V>();
+            TCG_CUDA(cudaMemcpyAsync(c->qtg.as<V>() + (size_t)(ntq + i) * N, chsrc + (size_t)Q.grid[i] * N,
+                                     N * sizeof(V), cudaMemcpyDeviceToDevice, c->stream));
+        }
+        double2 *accP = c->accP.as<double2>() + aoff[sq] * N;
+        const bool eqq = h.A[sq * 2 + 0] == h.A[sq * 2 + 1] && h.F[sq * 2 + 0] == h.F[sq * 2 + 1];
+        if (bitc && eqq) TRY((qp_pairs<T, true, true>(c, sq, ntq, Q.key, Q.cart, S, lo, hi, accP, nacc)));
+        else if (bitc) TRY((qp_pairs<T, true, false>(c, sq, ntq, Q.key, Q.cart, S, lo, hi, accP, nacc)));
+        else if (eqq) TRY((qp_pairs<T, false, true>(c, sq, ntq, Q.key, Q.cart, S, lo, hi, accP, nacc)));
+        else TRY((qp_pairs<T, false, false>(c, sq, ntq, Q.key, Q.cart, S, lo, hi, accP, nacc)));
+    }
+    TCG_CUDA(cudaStreamSynchronize(c->stream));
+    return TCG_OK;
+}
+
+// Second half, on the summed c->accP: G = 0 divergence correction of 3a2,
+// rotation of the intermediates to every equivalent q2, the 3a2 / 3b2 local
+// potentials and the rotated Qt / Bt grids of the band part
+// (tc3a2a4b2b5.cpp:496-817, :922-958).
+template <typename T>
+static int qp_finish(tcg_ctx *c)
 {
     PhaseScope ps_(c, "st:qp");
     using V = typename C2<T>::t;
@@ -905,6 +999,7 @@ static int qp_stage(tcg_ctx *c)
     memcpy(rc.R, h.recip, sizeof rc.R);
     const GridDesc &g = c->gd;
     const unsigned pblocks = (unsigned)std::min<size_t>(148 * 8, (N + 255) / 256);
+    const std::vector<size_t> aoff = qp_acc_offsets(c);
     TRY(c->Qt.ensure(h.nocc_grids * 3 * N * sizeof(V)));
     TRY(c->Bt.ensure(h.nocc_grids * 3 * N * sizeof(V)));
     TRY(c->V3a2.ensure((size_t)ns * N * sizeof(double2)));
@@ -915,42 +1010,13 @@ static int qp_stage(tcg_ctx *c)
     TRY(rot.ensure(6 * N * sizeof(double2)));
     DBuf &q3b2 = c->q3b2w;
     TRY(q3b2.ensure(3 * N * sizeof(double2)));
-    int rcode = TCG_OK;
-    for (int sq = 0; sq < ns && rcode == TCG_OK; sq++) {
+    for (int sq = 0; sq < ns; sq++) {
         TRY(launch(c, k_zero, dim3(pblocks), dim3(256), 0, q3b2.as<double2>(), 3 * N));
-        // targets: (iq2 irreducible, i2)
-        std::vector<int> tkey, tgrid;
-        std::vector<double> tcart;
-        for (int iq2 = 0; iq2 < h.nk; iq2++) {
-            double q[3];
-            cart(h, &h.kvec[3 * h.kall_off[iq2]], q);
-            for (int i = 0; i < h.nocc[sq * h.nk + iq2]; i++) {
-                tkey.push_back(iq2);
-                tgrid.push_back((int)(h.occ_off[(size_t)sq * h.nk_all + h.kall_off[iq2]] + i));
-                tcart.insert(tcart.end(), q, q + 3);
-            }
-        }
+        const QPTargets Q = qp_targets(c, sq);
+        const std::vector<int> &tkey = Q.key, &tgrid = Q.grid;
         const int ntq = (int)tkey.size();
         if (ntq == 0) continue;
-        Sources S = sources_of(c, sq);
-        // target grids are not contiguous in Rocc (isym > 0 grids in between):
-        // gather them into a contiguous copy
-        TRY(c->qtg.ensure((size_t)ntq * 2 * N * sizeof(V)));
-        for (int i = 0; i < ntq; i++) {
-            TCG_CUDA(cudaMemcpyAsync(c->qtg.as<V>() + (size_t)i * N, c->Rocc.as<V>() + (size_t)tgrid[i] * N,
-                                     N * sizeof(V), cudaMemcpyDeviceToDevice, c->stream));
-            const V *chsrc = bitc ? c->Rchi.as<V>() : c->Rocc.as<V>();
-            TCG_CUDA(cudaMemcpyAsync(c->qtg.as<V>() + (size_t)(ntq + i) * N, chsrc + (size_t)tgrid[i] * N,
-                                     N * sizeof(V), cudaMemcpyDeviceToDevice, c->stream));
-        }
-        TRY(c->accP.ensure((size_t)ntq * nacc * N * sizeof(double2)));
-        double2 *accP = c->accP.as<double2>();
-        TRY(launch(c, k_zero, dim3(148 * 8), dim3(256), 0, accP, (size_t)ntq * nacc * N));
-        const bool eqq = h.A[sq * 2 + 0] == h.A[sq * 2 + 1] && h.F[sq * 2 + 0] == h.F[sq * 2 + 1];
-        if (bitc && eqq) TRY((qp_pairs<T, true, true>(c, sq, ntq, tkey, tcart, S, accP, nacc)));
-        else if (bitc) TRY((qp_pairs<T, true, false>(c, sq, ntq, tkey, tcart, S, accP, nacc)));
-        else if (eqq) TRY((qp_pairs<T, false, true>(c, sq, ntq, tkey, tcart, S, accP, nacc)));
-        else TRY((qp_pairs<T, false, false>(c, sq, ntq, tkey, tcart, S, accP, nacc)));
+        double2 *accP = c->accP.as<double2>() + aoff[sq] * N;
         // B = -conj(Q) for TC, then forward FFTs of all accumulators
         if (!bitc)
             for (int i = 0; i < ntq; i++)
@@ -1082,8 +1148,17 @@ static int qp_stage(tcg_ctx *c)
     }
     TCG_CUDA(cudaStreamSynchronize(c->stream));
     h.qp_ready = true;
-    return rcode;
+    return TCG_OK;
 }
+
+template <typename T>
+static int qp_stage(tcg_ctx *c)
+{
+    TRY(qp_partial<T>(c, 0, 1));
+    return qp_finish<T>(c);
+}
+
+
 
 template <typename T>
 static int run_tc3a2a4b2b5_band(tcg_ctx *c, const Targets &Tg, double2 *acc)
@@ -1180,6 +1255,7 @@ static int state_terms(tcg_ctx *c)
     using V = typename C2<T>::t;
     Host &h = c->h;
     h.qp_ready = false;
+    h.qp_pending = false;
     if (h.method == TCG_METHOD_HF) return TCG_OK;
     const size_t N = h.N;
     const int ns = h.nspin;
@@ -1322,6 +1398,8 @@ static int apply_impl(tcg_ctx *c, const ApplyArgs &A)
         TRY(c->acc3.ensure(nt * N * sizeof(double2)));
         double2 *acc = c->acc3.as<double2>();
         TRY(launch(c, k_zero, dim3(pblocks), dim3(256), 0, acc, nt * N));
+        if ((m3 & TCG_TERM_TC3A2A4B2B5) && h.qp_pending)
+            return fail(TCG_ERR_STATE, "tcg_qp_partial was called: sum its buffer and call tcg_qp_finish first");
         if ((m3 & TCG_TERM_TC3A2A4B2B5) && !h.qp_ready) TRY(qp_stage<T>(c));
         // local potentials: tc3a1, tc3b1, and the 3a2 / 3b2 parts of tc3a2a4b2b5
         const double Nk = h.num_kpoints, Om = h.omega;

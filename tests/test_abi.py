@@ -55,20 +55,15 @@ def test_version_and_error_without_gpu(lib):
     assert e.value.code == 2            # TCG_ERR_CUDA: no device, no fallback
 
 
-def test_struct_layout_matches_header():
+def test_struct_layout_matches_header(tmp_path):
     """ctypes mirrors of the descriptors have the C sizes (compiled check)"""
     from tc_b200 import abi
-    src = os.path.join(ROOT, "_work_size_probe.c")
-    exe = os.path.join(ROOT, "_work_size_probe")
-    try:
-        open(src, "w").write('#include "include/tcg.h"\n#include <stdio.h>\n'
-                             'int main(){printf("%zu %zu\\n", sizeof(tcg_system_desc), sizeof(tcg_state_desc));}\n')
-        subprocess.run(["gcc", "-I", ROOT, "-o", exe, src], check=True, cwd=ROOT)
-        a, b = map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split())
-    finally:
-        for f in (src, exe):
-            if os.path.exists(f):
-                os.remove(f)
+    src = tmp_path / "size_probe.c"
+    exe = tmp_path / "size_probe"
+    src.write_text('#include "include/tcg.h"\n#include <stdio.h>\n'
+                   'int main(){printf("%zu %zu\\n", sizeof(tcg_system_desc), sizeof(tcg_state_desc));}\n')
+    subprocess.run(["gcc", "-I", ROOT, "-o", str(exe), str(src)], check=True)
+    a, b = map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split())
     assert C.sizeof(abi.SystemDesc) == a
     assert C.sizeof(abi.StateDesc) == b
 

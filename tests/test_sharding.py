@@ -1,7 +1,13 @@
-"""Band-apply sharding over ranks (bench.py --gpus N): world-size-2 gloo
-processes on CPU.  Each rank owns the bands of its k-points; the union of
-the ranks' partial H psi (oracle on CPU as the stand-in compute) must equal
-the unsharded result, and the max-over-ranks timing reduction is checked."""
+"""Multi-rank host logic (tc_b200.sharding, bench.py --gpus N) with
+world-size-2 gloo processes on CPU.
+- Band-apply sharding: each rank owns the bands of its k-points; the union of
+  the ranks' partial H psi (oracle on CPU as the stand-in compute) equals the
+  unsharded result, and the max-over-ranks timing reduction is checked.
+- Occupied-pair stage of tc3a2a4b2b5: the protocol of sharded_qp_stage
+  (partial share -> in-place all_reduce of the device buffer -> finish) on a
+  stand-in context whose buffer is a CPU tensor.  The numbers of the split
+  itself (partial grids of two ranks summing to the whole stage) are checked
+  on the GPU in tests/test_gpu_sharding.py."""
 import os
 import socket
 
@@ -25,12 +31,11 @@ def _worker(rank, world, port, q):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        import bench
-        from tc_b200 import abi, synth
+        from tc_b200 import abi, sharding, synth
         from oracle import oracle as O
         O.set_threads(1)
         s = synth.small("TC", nk=2)
-        own = bench.shard_owned(s, world, rank)
+        own = sharding.owned_mask(s, world, rank)
         h2, h3 = O.apply(s, abi.TERMS_TC, owned=own)
         t = torch.from_numpy(np.concatenate([h2.view(np.float64), h3.view(np.float64)]))
         dist.all_reduce(t)                               # union of disjoint shards
@@ -67,3 +72,54 @@ def test_two_rank_sharding_reproduces_full_apply():
     assert np.all(stack.sum(0) == 1)              # every band owned exactly once
     assert stack[0].sum() > 0 and stack[1].sum() > 0
     assert tmax == 2.0
+
+
+class _FakeCtx:
+    """stand-in for tc_b200.context.Context: the partial buffer of rank r holds
+    (r + 1) * [0, 1, 2, ...]; the calls are logged in order"""
+
+    def __init__(self, n):
+        import torch
+        self.buf = torch.zeros(n, dtype=torch.float64)
+        self.log = []
+
+    def qp_partial(self, rank, world):
+        import torch
+        self.log.append(("partial", rank, world))
+        self.buf[:] = (rank + 1) * torch.arange(self.buf.numel(), dtype=torch.float64)
+        return 12345, self.buf.numel() * 8
+
+    def qp_finish(self):
+        self.log.append(("finish", float(self.buf[1])))
+
+
+def _qp_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from tc_b200 import sharding
+        ctx = _FakeCtx(7)
+        sharding.sharded_qp_stage(ctx, view=lambda ptr, nbytes: ctx.buf)
+        q.put((rank, ctx.log, ctx.buf.numpy().copy()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_qp_stage_protocol():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_qp_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, log, buf in res:
+        # each rank computed its own share, then finished on the summed buffer
+        assert log == [("partial", rank, world), ("finish", 3.0)]
+        assert np.array_equal(buf, 3.0 * np.arange(7))

@@ -1,10 +1,12 @@
 """The allocation-free divergence-sum entry point (tcg_sum_of_vaux_noalloc)
 against the regular one (tcg_sum_of_vaux), on two calls in a row.
 
-Callers that cannot allocate device memory (stream capture, external pools)
-pass device inputs / outputs and the library works in a static device
-array.  This file is collected last so a failure here does not hide the
-other GPU tests; it must also pass alone in a fresh process."""
+Some hosts cannot allocate device memory from inside the library: their memory
+pool has reserved the GPU up front, or they must avoid the device-wide
+synchronisation that cudaMalloc / cudaFree imply.  They pass device inputs and
+outputs, and the library works in a static device array.  This file is
+collected last so that a failure here does not hide the other GPU tests; it
+also passes alone in a fresh process."""
 import numpy as np
 import pytest
 
@@ -23,10 +25,20 @@ def test_noalloc_matches_regular_twice(name):
     dev = torch.device("cuda", 0)
     kirr_t = torch.from_numpy(kirr).to(dev)
     kall_t = torch.from_numpy(np.ascontiguousarray(s.kvec)).to(dev)
-    for _ in range(2):
-        out = torch.full((s.nk_irr,), float("nan"), dtype=torch.float64, device=dev)
-        torch.cuda.synchronize()
+    # every output buffer exists before the free-memory reading, so that the
+    # only device work inside the window is the library's own
+    outs = [torch.full((s.nk_irr,), float("nan"), dtype=torch.float64, device=dev) for _ in range(3)]
+    torch.cuda.synchronize()
+    # warm-up: the first call on a device looks the static array up and may
+    # load the kernels' module; it is checked like the others
+    sum_of_vaux_noalloc(s, kirr_t.data_ptr(), kall_t.data_ptr(), outs[0].data_ptr())
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    for out in outs[1:]:
         alpha = sum_of_vaux_noalloc(s, kirr_t.data_ptr(), kall_t.data_ptr(), out.data_ptr())
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info(dev)[0] == free0, "device free memory changed across the call"
+    for out in outs:
         got = out.cpu().numpy()
         assert abs(alpha - alpha_ref) <= 1e-15 * abs(alpha_ref)
         assert np.all(np.isfinite(got))
