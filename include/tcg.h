@@ -78,6 +78,18 @@ extern "C" {
 #define TCG_TERMS_HF   (TCG_TERM_HF2X)
 #define TCG_TERMS_TC   (TCG_TERM_TC2X | TCG_TERM_TC3A1 | TCG_TERM_TC3B1 | \
                         TCG_TERM_TC3A2A4B2B5 | TCG_TERM_TC3A3B3B4B6)
+/* Hartree-type two-body terms (local potentials of the density, added to H2):
+ * hf2h (calc_hamiltonian_hf2h.cpp:7-85) for HF, tc2h
+ * (calc_hamiltonian_tc2h.cpp:10-235) for TC / BITC. */
+#define TCG_TERM_HF2H          (1u << 6)
+#define TCG_TERM_TC2H          (1u << 7)
+/* One-body terms, applied by tcg_apply_h1 into H1: kinetic
+ * (calc_hamiltonian_kinetic.cpp:6-52) and pseudopotential, local + non-local
+ * (calc_hamiltonian_pseudo.cpp:6-180; data from tcg_set_pseudo). */
+#define TCG_TERM_KINETIC       (1u << 8)
+#define TCG_TERM_PSEUDO        (1u << 9)
+#define TCG_TERMS_H1   (TCG_TERM_KINETIC | TCG_TERM_PSEUDO)
+#define TCG_TERMS_H2   (TCG_TERM_HF2X | TCG_TERM_TC2X | TCG_TERM_HF2H | TCG_TERM_TC2H)
 
 /* ---- static system description (one per run) ----------------------------
  * "nk_all" below is sum_k nsym_k (Kpoints::num_kpoints_all_scf).  Arrays
@@ -123,6 +135,23 @@ typedef struct tcg_state_desc {
     const double  *density;      /* [2][N] complex, R-space (set_density)       */
 } tcg_state_desc;
 
+/* ---- pseudopotential (Potentials, one per run) ---------------------------
+ * What calc_hamiltonian::pseudo reads (calc_hamiltonian_pseudo.cpp:6-180):
+ * the local potential on the FFT grid and, per irreducible k, the non-local
+ * projectors <beta|k+G> of every species as Potentials::projector_nonlocal
+ * returns them (without the exp(i G.R_atom) factor, which is applied here). */
+typedef struct tcg_pseudo_desc {
+    const double  *vloc;            /* [N] Potentials::Vpp_local (real, R space) or NULL */
+    int32_t nspecies, natoms;
+    const int32_t *species_of_atom; /* [natoms] CrystalStructure::index_of_atoms */
+    const double  *atom_pos;        /* [natoms][3] atomic_position_cartesian (bohr) */
+    const int32_t *nproj;           /* [nspecies] pseudo_lbeta[is].size()          */
+    const int32_t *lbeta;           /* [sum nproj] pseudo_lbeta                     */
+    const double  *dij;             /* [sum nproj^2] pseudo_dij[is](i, j) row-major */
+    const double  *projector;       /* complex [nk_irr][sum_is sum_ip (2 l + 1)][npw of k]:
+                                       projector[is][ip][m] at the isym-0 plane waves of k */
+} tcg_pseudo_desc;
+
 /* Opaque context: device copies of the system and state, FFT plans, scratch. */
 typedef struct tcg_ctx tcg_ctx;
 
@@ -146,7 +175,8 @@ int tcg_refresh_state(tcg_ctx *ctx);
 
 /* Apply the selected terms to a block of trial orbitals and ACCUMULATE into
  * h2 / h3 (the reference's "+=" semantics; the caller zeroes them first as
- * calc_hamiltonian_all.cpp:29-49 does).
+ * calc_hamiltonian_all.cpp:29-49 does).  H2 terms: hf2x, hf2h (HF) or tc2x,
+ * tc2h (TC / BITC); H3 terms: the four tc3* routines.
  *   nb_apply : [nspin][nk_irr] bands per (spin, k)  (H2phi[ispin][ik].size())
  *   psi      : [nspin][nk_irr][nb_apply][npw] complex, packed
  *   h2, h3   : same layout as psi; h3 may be NULL for HF, h2 NULL if no
@@ -158,6 +188,18 @@ int tcg_refresh_state(tcg_ctx *ctx);
  * tc3a2a4b2b5 / tc3a3b3b4b6 (calc_hamiltonian.hpp:54-130). */
 int tcg_apply(tcg_ctx *ctx, uint32_t term_mask, const int32_t *nb_apply,
               const double *psi, double *h2, double *h3, const uint8_t *owned);
+
+/* One-body terms (TCG_TERM_KINETIC, TCG_TERM_PSEUDO) applied to psi and
+ * ACCUMULATED into h1 (host pointers, layout of tcg_apply).  Replaces
+ * calc_hamiltonian::kinetic (calc_hamiltonian_kinetic.cpp:6-52) and
+ * calc_hamiltonian::pseudo (calc_hamiltonian_pseudo.cpp:6-180); the
+ * pseudopotential needs tcg_set_pseudo first. */
+int tcg_apply_h1(tcg_ctx *ctx, uint32_t term_mask, const int32_t *nb_apply,
+                 const double *psi, double *h1, const uint8_t *owned);
+
+/* Upload the pseudopotential data (once per run).  Fails with TCG_ERR_ARG
+ * if pseudo_dij couples projectors of different l (as the reference). */
+int tcg_set_pseudo(tcg_ctx *ctx, const tcg_pseudo_desc *pp);
 
 /* Same as tcg_apply but psi / h2 / h3 are DEVICE pointers (layout as above)
  * and the work is queued on the context's stream without a host sync. */
@@ -177,6 +219,25 @@ int tcg_apply_device(tcg_ctx *ctx, uint32_t term_mask, const int32_t *nb_apply,
  * skipped.  e_out[4] = {Re E2, Im E2, Re E3, Im E3} (host).  The sum runs in a
  * fixed order: repeated calls give identical bits. */
 int tcg_energy(tcg_ctx *ctx, const int32_t *nb_apply, const void *h2_dev, const void *h3_dev, double *e_out);
+
+/* Backward pass: energy gradients of the current state (no reference
+ * counterpart -- TC++ has no adjoint).  E = E2 + E3 as tcg_energy, with H
+ * (the terms of term_mask) applied to the occupied right orbitals and built
+ * from those same orbitals and the state's density (for a variational
+ * gradient, the density of these orbitals, e.g. from tcg_density).
+ *   e_out[4]     E2, E3 (re, im)
+ *   dE_dchi_dev  DEVICE [nspin][nk][nbands[s]][npw] complex (the layout of
+ *                phik_left) or NULL: dE / d conj(chi_i)(G) = f_i / N_k
+ *                (H2 + H3) phi_i(G) for the occupied bands, 0 for the others
+ *                (E is a polynomial in conj(chi) and H2, H3 are its
+ *                mean-field derivatives).  Needs nsym_k = 1 for every k.
+ *   dE_du, dE_dv2  host [nspin][N] complex each, or NULL: the tc2x part of
+ *                dE/du(G; s, s) and dE/dV_2body(G; s, s) on the FFT grid,
+ *                from pair densities recomputed block by block (never all
+ *                stored).  Gamma-only systems, TCG_TERM_TC2X in term_mask.
+ * Fails with TCG_ERR_UNSUPPORTED outside these limits. */
+int tcg_energy_grad(tcg_ctx *ctx, uint32_t term_mask, double *e_out, void *dE_dchi_dev, double *dE_du,
+                    double *dE_dv2);
 
 /* Divergence-correction scalars for the SCF mesh (Potentials::set_sum_of_Vaux
  * with set_sum_of_Vaux_each, potentials_coulomb.cpp:60-161), computed on the

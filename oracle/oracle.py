@@ -31,6 +31,8 @@ def lib():
         L = C.CDLL(SO)
         L.tco_apply.argtypes = [C.POINTER(abi.SystemDesc), C.POINTER(abi.StateDesc), C.c_uint32,
                                 C.POINTER(C.c_int32), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.tco_apply_h1.argtypes = [C.POINTER(abi.SystemDesc), C.POINTER(abi.PseudoDesc), C.c_uint32,
+                                   C.POINTER(C.c_int32), C.c_void_p, C.c_void_p, C.c_void_p]
         L.tco_density.argtypes = [C.POINTER(abi.SystemDesc), C.POINTER(abi.StateDesc), C.c_void_p]
         L.tco_sum_of_vaux.argtypes = [C.POINTER(abi.SystemDesc), C.POINTER(C.c_double), C.c_void_p]
         L.tco_fft3d.argtypes = [C.POINTER(C.c_int32), C.c_void_p, C.c_int]
@@ -80,6 +82,20 @@ def apply(sysm, mask, psi=None, nb_apply=None, owned=None):
                            nb.ctypes.data_as(C.POINTER(C.c_int32)), psi.ctypes.data, h2.ctypes.data,
                            h3.ctypes.data, None if own is None else own.ctypes.data))
     return h2, h3
+
+
+def apply_h1(sysm, mask, pseudo=None, psi=None, nb_apply=None, owned=None):
+    """h1 = oracle one-body terms (kinetic, pseudopotential) applied to psi."""
+    sysd, _, keep = sysm.descriptors()
+    pd, pkeep = (None, None) if pseudo is None else pseudo.descriptor()
+    nb = np.ascontiguousarray(sysm.nb_apply if nb_apply is None else nb_apply, dtype=np.int32)
+    psi = np.ascontiguousarray(sysm.psi if psi is None else psi, dtype=np.complex128)
+    h1 = np.zeros_like(psi)
+    own = None if owned is None else np.ascontiguousarray(owned, dtype=np.uint8)
+    _check(lib().tco_apply_h1(C.byref(sysd), None if pd is None else C.byref(pd), C.c_uint32(mask),
+                              nb.ctypes.data_as(C.POINTER(C.c_int32)), psi.ctypes.data, h1.ctypes.data,
+                              None if own is None else own.ctypes.data))
+    return h1
 
 
 def density(sysm):

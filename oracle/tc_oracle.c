@@ -721,6 +721,195 @@ static void run_tc3b1(const octx *c, const packing *P, const task *T, int nt, co
 }
 
 /* ======================================================================
+ * Hartree-type two-body terms: hf2h (calc_hamiltonian_hf2h.cpp:7-85) and
+ * tc2h (calc_hamiltonian_tc2h.cpp:10-235)
+ * ====================================================================== */
+static void run_hf2h(const octx *c, const packing *P, const task *T, int nt, const cplx *psi, cplx *h2)
+{
+    const double f = 1.0 / (c->sys->num_kpoints * c->sys->omega);   /* :32 */
+    cplx *V = gnew(c);
+    for (int i = 0; i < c->N; i++) V[i] = dens(c, 0)[i] + dens(c, 1)[i];   /* :40 */
+    fft3_exec(&c->F, V, 1);
+    V[0] = 0.0;                                                               /* :42 */
+    for (int i = 1; i < c->N; i++) {
+        const double *G = c->Gv[i];
+        V[i] *= FOURPI / (G[0] * G[0] + G[1] * G[1] + G[2] * G[2]);
+    }
+    fft3_exec(&c->F, V, 0);
+    cplx *Vs[2] = {V, V};
+    apply_local(c, P, T, nt, psi, h2, Vs, f);                                /* :64-80 */
+    free(V);
+}
+
+static void run_tc2h(const octx *c, const packing *P, const task *T, int nt, const cplx *psi, cplx *h2)
+{
+    const int N = c->N, ns = c->nspin;
+    const double f = 1.0 / (c->sys->num_kpoints * c->sys->omega);         /* :28 */
+    /* [2b_h2] phiq_gphiq[s][d] = sum_q f conj(chi_q(r)) grad_d phi_q(r), to G (:53-140) */
+    cplx *pg[2][3] = {{0}};
+    cplx *orb = gnew(c), *gr = gnew(c);
+    for (int s = 0; s < ns; s++) {
+        for (int d = 0; d < 3; d++) pg[s][d] = gnew(c);
+        for (int a = 0; a < c->nk_all; a++) {
+            const int ik = c->ik_of_all[a];
+            double q[3];
+            cart(c->sys, c->sys->kvec + 3 * a, q);
+            for (int i = 0; i < nocc(c, s, ik); i++) {
+                const double fq = fill(c, s, ik, i);
+                scatter(c, s, a, phik_band(c, s, ik, i), orb);
+                const cplx *chr = Rchi(c, s, a, i);
+                for (int d = 0; d < 3; d++) {
+                    for (int p = 0; p < N; p++) gr[p] = (q[d] + c->Gv[p][d]) * orb[p];
+                    fft3_exec(&c->F, gr, 0);
+                    for (int p = 0; p < N; p++) pg[s][d][p] += fq * conj(chr[p]) * gr[p];
+                }
+            }
+        }
+        for (int d = 0; d < 3; d++) fft3_exec(&c->F, pg[s][d], 1);
+    }
+    /* [2a_h + 2b_h2] V_2body[s], [2b_h1] dnu[s][d] (:142-186) */
+    cplx *V[2] = {0, 0}, *dn[2][3] = {{0}};
+    const double spin_factor = ns == 1 ? 2.0 : 1.0;
+    for (int s = 0; s < ns; s++) {
+        V[s] = gnew(c);
+        for (int d = 0; d < 3; d++) dn[s][d] = gnew(c);
+        for (int js = 0; js < 2; js++) {
+            const int jr = ns == 1 ? 0 : js;
+            memcpy(orb, dens(c, js), sizeof(cplx) * N);
+            fft3_exec(&c->F, orb, 1);
+            for (int p = 0; p < N; p++) {
+                const double *G = c->Gv[p];
+                V[s][p] += tco_tc2body(c->sys, G, s, js) * orb[p];
+                const double u = tco_uk(c->sys, G, s, js);
+                for (int d = 0; d < 3; d++) {
+                    V[s][p] += u * G[d] * pg[jr][d][p] / spin_factor;
+                    dn[s][d][p] += u * G[d] * orb[p];
+                }
+            }
+        }
+        fft3_exec(&c->F, V[s], 0);
+        for (int d = 0; d < 3; d++) fft3_exec(&c->F, dn[s][d], 0);
+    }
+    free(orb);
+    free(gr);
+    /* per band: V_2body phi - sum_d grad_d phi dnu_d (:188-233) */
+#pragma omp parallel for schedule(dynamic, 1) num_threads(tco_get_threads())
+    for (int t = 0; t < nt; t++) {
+        const int s = T[t].s, ik = T[t].ik, j = T[t].j;
+        double k[3];
+        cart(c->sys, c->sys->kvec + 3 * a0(c, ik), k);
+        cplx *o = gnew(c), *g = gnew(c), *vo = gnew(c);
+        scatter(c, s, a0(c, ik), psi + pk(P, c, s, ik, j), o);
+        for (int d = 0; d < 3; d++) {
+            for (int p = 0; p < N; p++) g[p] = (k[d] + c->Gv[p][d]) * o[p];
+            fft3_exec(&c->F, g, 0);
+            for (int p = 0; p < N; p++) vo[p] -= g[p] * dn[s][d][p];
+        }
+        fft3_exec(&c->F, o, 0);
+        for (int p = 0; p < N; p++) vo[p] += V[s][p] * o[p];
+        fft3_exec(&c->F, vo, 1);
+        gather_add(c, s, ik, vo, f, h2 + pk(P, c, s, ik, j));
+        free(o); free(g); free(vo);
+    }
+    for (int s = 0; s < ns; s++) {
+        free(V[s]);
+        for (int d = 0; d < 3; d++) { free(dn[s][d]); free(pg[s][d]); }
+    }
+}
+
+/* ======================================================================
+ * one-body terms: kinetic (calc_hamiltonian_kinetic.cpp:6-52) and
+ * pseudopotential (calc_hamiltonian_pseudo.cpp:6-180)
+ * ====================================================================== */
+static void run_kinetic(const octx *c, const packing *P, const task *T, int nt, const cplx *psi, cplx *h1)
+{
+    for (int t = 0; t < nt; t++) {
+        const int s = T[t].s, ik = T[t].ik, j = T[t].j;
+        double k[3];
+        cart(c->sys, c->sys->kvec + 3 * a0(c, ik), k);
+        const int32_t *gi = c->sys->gindex + gidx_offset(c, s, a0(c, ik));
+        const cplx *ps = psi + pk(P, c, s, ik, j);
+        cplx *h = h1 + pk(P, c, s, ik, j);
+        for (int p = 0; p < c->sys->npw[ik]; p++) {
+            double kg2 = 0;
+            for (int d = 0; d < 3; d++) kg2 += (k[d] + c->Gv[gi[p]][d]) * (k[d] + c->Gv[gi[p]][d]);
+            h[p] += 0.5 * kg2 * ps[p];                                  /* :38-41 */
+        }
+    }
+}
+
+static int run_pseudo(const octx *c, const tcg_pseudo_desc *pp, const packing *P, const task *T, int nt,
+                      const cplx *psi, cplx *h1)
+{
+    /* component offsets (species, projector) -> first m, and per-k offsets */
+    for (int is = 0; is < pp->nspecies; is++)
+        if (pp->nproj[is] > 64) return fail(TCG_ERR_UNSUPPORTED, "more than 64 projectors per species");
+    int ncomp = 0, *coff = malloc(sizeof(int) * 64 * (pp->nspecies > 0 ? pp->nspecies : 1));
+    int *poff = malloc(sizeof(int) * (pp->nspecies + 1)), *doff = malloc(sizeof(int) * (pp->nspecies + 1));
+    poff[0] = doff[0] = 0;
+    for (int is = 0; is < pp->nspecies; is++) {
+        poff[is + 1] = poff[is] + pp->nproj[is];
+        doff[is + 1] = doff[is] + pp->nproj[is] * pp->nproj[is];
+        for (int ip = 0; ip < pp->nproj[is]; ip++) {
+            coff[64 * is + ip] = ncomp;
+            ncomp += 2 * pp->lbeta[poff[is] + ip] + 1;
+        }
+    }
+    size_t *koff = malloc(sizeof(size_t) * (c->nk + 1));
+    koff[0] = 0;
+    for (int k = 0; k < c->nk; k++) koff[k + 1] = koff[k] + (size_t)ncomp * c->sys->npw[k];
+    int bad = 0;
+    for (int t = 0; t < nt && !bad; t++) {
+        const int s = T[t].s, ik = T[t].ik, j = T[t].j;
+        const int npw = c->sys->npw[ik];
+        const int32_t *gi = c->sys->gindex + gidx_offset(c, s, a0(c, ik));
+        const cplx *ps = psi + pk(P, c, s, ik, j);
+        cplx *h = h1 + pk(P, c, s, ik, j);
+        const cplx *proj = (const cplx *)pp->projector + koff[ik];
+        cplx *ph = malloc(sizeof(cplx) * npw);
+        /* (1/2) non-local part (:120-160) */
+        for (int ia = 0; ia < pp->natoms && !bad; ia++) {
+            const int is = pp->species_of_atom[ia];
+            const double *R = pp->atom_pos + 3 * ia;
+            for (int p = 0; p < npw; p++) {
+                const double *G = c->Gv[gi[p]];   /* G without k (:130-134) */
+                const double arg = G[0] * R[0] + G[1] * R[1] + G[2] * R[2];
+                ph[p] = cos(arg) + I * sin(arg);
+            }
+            for (int jp = 0; jp < pp->nproj[is]; jp++) {
+                const int lb = pp->lbeta[poff[is] + jp];
+                for (int im = 0; im < 2 * lb + 1; im++) {
+                    const cplx *pj = proj + (size_t)(coff[64 * is + jp] + im) * npw;
+                    cplx coeff = 0;
+                    for (int p = 0; p < npw; p++) coeff += ph[p] * pj[p] * ps[p];
+                    for (int ip = 0; ip < pp->nproj[is]; ip++) {
+                        const double D = pp->dij[doff[is] + ip * pp->nproj[is] + jp];
+                        if (fabs(D) > 1e-8) {
+                            if (pp->lbeta[poff[is] + ip] != lb) { bad = 1; break; }
+                            const cplx *pi = proj + (size_t)(coff[64 * is + ip] + im) * npw;
+                            for (int p = 0; p < npw; p++) h[p] += D * coeff * conj(ph[p] * pi[p]);
+                        }
+                    }
+                }
+            }
+        }
+        free(ph);
+        /* (2/2) local part (:163-175) */
+        if (pp->vloc && !bad) {
+            cplx *o = gnew(c);
+            scatter(c, s, a0(c, ik), ps, o);
+            fft3_exec(&c->F, o, 0);
+            for (int p = 0; p < c->N; p++) o[p] *= pp->vloc[p];
+            fft3_exec(&c->F, o, 1);
+            gather_add(c, s, ik, o, 1.0, h);
+            free(o);
+        }
+    }
+    free(coff); free(poff); free(doff); free(koff);
+    return bad ? fail(TCG_ERR_ARG, "dij is not diagonal w.r.t. l in pseudopot.") : TCG_OK;
+}
+
+/* ======================================================================
  * tc3a3b3b4b6 -- calc_hamiltonian_tc3a3b3b4b6.cpp:11-863 (kVaux = 0)
  * ====================================================================== */
 static int kpoint_on_mesh(const octx *c, int ik)
@@ -1014,26 +1203,31 @@ static void run_tc3a2a4b2b5(const octx *c, const packing *P, const task *T, int 
             double q2v[3];
             cart(c->sys, c->sys->kvec + 3 * a0(c, iq2), q2v);
             /* occupied-pair stage (:210-443): accumulators per (i2, part) */
-            const int nparts = nthr < c->nk_all ? nthr : c->nk_all;
+            /* the visited source k-points (all of them, or every qstride-th in the
+             * timing-sample mode), split evenly over the parts */
+            int *alist = malloc(sizeof(int) * c->nk_all), nal = 0;
+            for (int a1 = 0; a1 < c->nk_all; a1++)
+                if (nocc(c, sq, c->ik_of_all[a1]) > 0 && !QSKIP(a1)) alist[nal++] = a1;
+            const int nparts = nal == 0 ? 1 : (nthr < nal ? nthr : nal);
             const int nacc = ns + 3 + (bitc ? 3 : 0);
             cplx *acc = calloc((size_t)no2 * nparts * nacc * N, sizeof(cplx));
-            if (!acc) return;
+            if (!acc) { free(alist); return; }
 #pragma omp parallel for collapse(2) schedule(dynamic, 1) num_threads(nthr)
             for (int i2 = 0; i2 < no2; i2++)
                 for (int part = 0; part < nparts; part++) {
                     cplx *A = acc + ((size_t)i2 * nparts + part) * nacc * N;
                     cplx *q3a2[2] = {A, ns > 1 ? A + N : A};
                     cplx *q3a4 = A + (size_t)ns * N, *q3b5 = A + (size_t)(ns + 3) * N;
-                    const int abeg = (int)((long)c->nk_all * part / nparts);
-                    const int aend = (int)((long)c->nk_all * (part + 1) / nparts);
+                    const int abeg = (int)((long)nal * part / nparts);
+                    const int aend = (int)((long)nal * (part + 1) / nparts);
                     const cplx *phiq2 = Rphi(c, sq, a0(c, iq2), i2), *chiq2 = Rchi(c, sq, a0(c, iq2), i2);
                     cplx *phiphi = gnew(c), *phij = gnew(c), *orb = gnew(c), *orb2 = gnew(c);
                     double *du[2][3];
                     for (int x = 0; x < 2; x++)
                         for (int d = 0; d < 3; d++) du[x][d] = malloc(sizeof(double) * N);
-                    for (int a1 = abeg; a1 < aend; a1++) {
+                    for (int ia = abeg; ia < aend; ia++) {
+                        const int a1 = alist[ia];
                         const int iq1 = c->ik_of_all[a1];
-                        if (nocc(c, sq, iq1) == 0 || QSKIP(a1)) continue;
                         double q1v[3], qq[3];
                         cart(c->sys, c->sys->kvec + 3 * a1, q1v);
                         for (int d = 0; d < 3; d++) qq[d] = q2v[d] - q1v[d];
@@ -1211,6 +1405,7 @@ static void run_tc3a2a4b2b5(const octx *c, const packing *P, const task *T, int 
                 for (int d = 0; d < 3; d++) { free(Q[d]); free(B[d]); }
             }
             free(acc);
+            free(alist);
         }
         /* 3b2 (:922-992) */
         for (int d = 0; d < 3; d++) fft3_exec(&c->F, qsum3b2[d], 1);
@@ -1263,10 +1458,11 @@ int tco_apply(const tcg_system_desc *sys, const tcg_state_desc *st, uint32_t mas
     if (rc) return rc;
     if (!nb_apply || !psi) return fail(TCG_ERR_ARG, "missing psi");
     const int is_hf = sys->calc_method == TCG_METHOD_HF;
-    if (is_hf && (mask & ~TCG_TERMS_HF)) return fail(TCG_ERR_ARG, "TC terms requested for HF");
-    if (!is_hf && (mask & TCG_TERM_HF2X)) return fail(TCG_ERR_ARG, "hf2x requested for TC/BITC");
-    if ((mask & (TCG_TERM_HF2X | TCG_TERM_TC2X)) && !h2) return fail(TCG_ERR_ARG, "h2 is NULL");
-    if ((mask & ~(TCG_TERM_HF2X | TCG_TERM_TC2X)) && !h3) return fail(TCG_ERR_ARG, "h3 is NULL");
+    if (mask & ~(TCG_TERMS_TC | TCG_TERMS_H2)) return fail(TCG_ERR_ARG, "unknown term bits");
+    if (is_hf && (mask & ~(TCG_TERM_HF2X | TCG_TERM_HF2H))) return fail(TCG_ERR_ARG, "TC terms requested for HF");
+    if (!is_hf && (mask & (TCG_TERM_HF2X | TCG_TERM_HF2H))) return fail(TCG_ERR_ARG, "HF terms requested for TC/BITC");
+    if ((mask & TCG_TERMS_H2) && !h2) return fail(TCG_ERR_ARG, "h2 is NULL");
+    if ((mask & ~TCG_TERMS_H2) && !h3) return fail(TCG_ERR_ARG, "h3 is NULL");
     if (sys->nsymop > 0 && (!sys->rotation || !sys->translation || !sys->rot_index))
         return fail(TCG_ERR_ARG, "missing symmetry arrays");
     const double t0 = now_s();
@@ -1280,6 +1476,8 @@ int tco_apply(const tcg_system_desc *sys, const tcg_state_desc *st, uint32_t mas
     int nt = make_tasks(&c, &P, owned, &T);
     const cplx *ps = (const cplx *)psi;
     if (mask & TCG_TERM_HF2X) run_hf2x(&c, &P, T, nt, ps, (cplx *)h2);
+    if (mask & TCG_TERM_HF2H) run_hf2h(&c, &P, T, nt, ps, (cplx *)h2);
+    if (mask & TCG_TERM_TC2H) run_tc2h(&c, &P, T, nt, ps, (cplx *)h2);
     if (mask & TCG_TERM_TC2X) run_tc2x(&c, &P, T, nt, ps, (cplx *)h2);
     if (mask & TCG_TERM_TC3A1) run_tc3a1(&c, &P, T, nt, ps, (cplx *)h3);
     if (mask & TCG_TERM_TC3B1) run_tc3b1(&c, &P, T, nt, ps, (cplx *)h3);
@@ -1290,6 +1488,28 @@ int tco_apply(const tcg_system_desc *sys, const tcg_state_desc *st, uint32_t mas
     ctx_free(&c);
     g_t_total += now_s() - t0;
     return TCG_OK;
+}
+
+int tco_apply_h1(const tcg_system_desc *sys, const tcg_pseudo_desc *pp, uint32_t mask, const int32_t *nb_apply,
+                 const double *psi, double *h1, const uint8_t *owned)
+{
+    if (!sys || !nb_apply || !psi || !h1) return fail(TCG_ERR_ARG, "null argument");
+    if (mask & ~TCG_TERMS_H1) return fail(TCG_ERR_ARG, "only one-body terms here");
+    if ((mask & TCG_TERM_PSEUDO) && !pp) return fail(TCG_ERR_ARG, "pseudopotential data missing");
+    octx c;
+    int rc = ctx_init(&c, sys, NULL, 0);
+    if (rc) { ctx_free(&c); return rc; }
+    packing P;
+    pack_init(&P, &c, nb_apply);
+    task *T;
+    int nt = make_tasks(&c, &P, owned, &T);
+    const cplx *ps = (const cplx *)psi;
+    if (mask & TCG_TERM_KINETIC) run_kinetic(&c, &P, T, nt, ps, (cplx *)h1);
+    if (mask & TCG_TERM_PSEUDO) rc = run_pseudo(&c, pp, &P, T, nt, ps, (cplx *)h1);
+    free(T);
+    free(P.off);
+    ctx_free(&c);
+    return rc;
 }
 
 /* BlochStates::set_density (bloch_states_scfloop_filling_density.cpp:256-360) */

@@ -34,11 +34,16 @@ int tco_fft3d(const int32_t nr[3], double *grid, int forward);
 double tco_uk(const tcg_system_desc *sys, const double G[3], int s1, int s2);
 double tco_tc2body(const tcg_system_desc *sys, const double G[3], int s1, int s2);
 
-/* calc_hamiltonian::{hf2x,tc2x,tc3a1,tc3b1,tc3a2a4b2b5,tc3a3b3b4b6}
- * restated; arguments as tcg_apply (accumulating into h2 / h3). */
+/* calc_hamiltonian::{hf2x,hf2h,tc2x,tc2h,tc3a1,tc3b1,tc3a2a4b2b5,
+ * tc3a3b3b4b6} restated; arguments as tcg_apply (accumulating into h2 / h3). */
 int tco_apply(const tcg_system_desc *sys, const tcg_state_desc *st,
               uint32_t term_mask, const int32_t *nb_apply,
               const double *psi, double *h2, double *h3, const uint8_t *owned);
+
+/* calc_hamiltonian::kinetic / pseudo restated (TCG_TERM_KINETIC,
+ * TCG_TERM_PSEUDO), accumulating into h1; pp may be NULL without PSEUDO. */
+int tco_apply_h1(const tcg_system_desc *sys, const tcg_pseudo_desc *pp, uint32_t term_mask,
+                 const int32_t *nb_apply, const double *psi, double *h1, const uint8_t *owned);
 
 /* BlochStates::set_density, first SCF iteration. */
 int tco_density(const tcg_system_desc *sys, const tcg_state_desc *st, double *density_out);

@@ -47,6 +47,9 @@ def lib():
                                               C.POINTER(C.c_double), vp]
         L.tcg_qp_partial.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(vp), C.POINTER(C.c_size_t)]
         L.tcg_qp_finish.argtypes = [vp]
+        L.tcg_set_pseudo.argtypes = [vp, C.POINTER(abi.PseudoDesc)]
+        L.tcg_apply_h1.argtypes = [vp, C.c_uint32, C.POINTER(C.c_int32), vp, vp, vp]
+        L.tcg_energy_grad.argtypes = [vp, C.c_uint32, C.POINTER(C.c_double), vp, vp, vp]
         L.tcg_energy.argtypes = [vp, C.POINTER(C.c_int32), vp, vp, C.POINTER(C.c_double)]
         _lib = L
     return _lib
@@ -60,4 +63,4 @@ def check(rc):
 EXPORTS = ["tcg_ctx_create", "tcg_ctx_destroy", "tcg_set_state", "tcg_apply", "tcg_apply_device",
            "tcg_sum_of_vaux", "tcg_density", "tcg_stream", "tcg_launch_count", "tcg_last_error",
            "tcg_version", "tcg_set_tuning", "tcg_profile", "tcg_profile_read", "tcg_refresh_state",
-           "tcg_sum_of_vaux_noalloc", "tcg_energy", "tcg_qp_partial", "tcg_qp_finish"]
+           "tcg_sum_of_vaux_noalloc", "tcg_energy", "tcg_qp_partial", "tcg_qp_finish", "tcg_set_pseudo", "tcg_apply_h1", "tcg_energy_grad"]

@@ -27,7 +27,12 @@ TERM_TC3A2A4B2B5 = 1 << 4
 TERM_TC3A3B3B4B6 = 1 << 5
 TERMS_HF = TERM_HF2X
 TERMS_TC = TERM_TC2X | TERM_TC3A1 | TERM_TC3B1 | TERM_TC3A2A4B2B5 | TERM_TC3A3B3B4B6
-TERMS_H2 = TERM_HF2X | TERM_TC2X
+TERM_HF2H = 1 << 6
+TERM_TC2H = 1 << 7
+TERM_KINETIC = 1 << 8
+TERM_PSEUDO = 1 << 9
+TERMS_H1 = TERM_KINETIC | TERM_PSEUDO
+TERMS_H2 = TERM_HF2X | TERM_TC2X | TERM_HF2H | TERM_TC2H
 TERM_NAMES = {
     "hf2x": TERM_HF2X,
     "tc2x": TERM_TC2X,
@@ -36,6 +41,8 @@ TERM_NAMES = {
     "tc3a2a4b2b5": TERM_TC3A2A4B2B5,
     "tc3a3b3b4b6": TERM_TC3A3B3B4B6,
 }
+# terms outside the exchange / three-body hot path (Hartree-type and one-body)
+TERM_NAMES_EXTRA = {"hf2h": TERM_HF2H, "tc2h": TERM_TC2H, "kinetic": TERM_KINETIC, "pseudo": TERM_PSEUDO}
 
 _i32p = C.POINTER(C.c_int32)
 _u8p = C.POINTER(C.c_uint8)
@@ -78,6 +85,20 @@ class StateDesc(C.Structure):
         ("phik", _f64p),
         ("phik_left", _f64p),
         ("density", _f64p),
+    ]
+
+
+class PseudoDesc(C.Structure):
+    _fields_ = [
+        ("vloc", _f64p),
+        ("nspecies", C.c_int32),
+        ("natoms", C.c_int32),
+        ("species_of_atom", _i32p),
+        ("atom_pos", _f64p),
+        ("nproj", _i32p),
+        ("lbeta", _i32p),
+        ("dij", _f64p),
+        ("projector", _f64p),
     ]
 
 

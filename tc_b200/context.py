@@ -24,7 +24,7 @@ def _terms(terms):
         terms = [terms]
     m = 0
     for t in terms:
-        m |= abi.TERM_NAMES[t]
+        m |= abi.TERM_NAMES[t] if t in abi.TERM_NAMES else abi.TERM_NAMES_EXTRA[t]
     return m
 
 
@@ -141,6 +141,20 @@ class Context:
     def qp_finish(self):
         check(lib().tcg_qp_finish(self.handle))
 
+    def energy_grad(self, terms, dchi_ptr=0, tables=False):
+        """(E2, E3, dE_du, dE_dv2) of the current state (tcg_energy_grad); dchi_ptr:
+        device buffer (layout of phik_left) for dE/d conj(chi), 0 to skip;
+        tables: also the tc2x Jastrow-table gradients [nspin][N] (Gamma only)."""
+        s = self.system
+        e = (C.c_double * 4)()
+        du = dv = None
+        if tables:
+            du = np.zeros((s.nspin, s.N), dtype=np.complex128)
+            dv = np.zeros((s.nspin, s.N), dtype=np.complex128)
+        check(lib().tcg_energy_grad(self.handle, C.c_uint32(_terms(terms)), e, C.c_void_p(dchi_ptr or None),
+                                    None if du is None else du.ctypes.data, None if dv is None else dv.ctypes.data))
+        return complex(e[0], e[1]), complex(e[2], e[3]), du, dv
+
     def energy_device(self, h2_ptr, h3_ptr, nb_apply=None):
         """(E2, E3) of the applied bands from DEVICE arrays h2 / h3 (packed like
         psi; pointers as ints, 0 = skip), reduced on the GPU in FP64."""
@@ -150,6 +164,23 @@ class Context:
         check(lib().tcg_energy(self.handle, nb.ctypes.data_as(C.POINTER(C.c_int32)), C.c_void_p(h2_ptr or None),
                                C.c_void_p(h3_ptr or None), out))
         return complex(out[0], out[1]), complex(out[2], out[3])
+
+    def set_pseudo(self, pseudo):
+        """Upload pseudopotential data (tc_b200.system.Pseudo) for the one-body terms."""
+        d, keep = pseudo.descriptor()
+        check(lib().tcg_set_pseudo(self.handle, C.byref(d)))
+        self._pseudo_keep = keep
+
+    def apply_h1(self, terms, psi=None, nb_apply=None, h1=None, owned=None):
+        """One-body terms (kinetic, pseudo) on host arrays; returns h1 with h1 += terms(psi)."""
+        s = self.system
+        nb = np.ascontiguousarray(s.nb_apply if nb_apply is None else nb_apply, dtype=np.int32)
+        psi = np.ascontiguousarray(s.psi if psi is None else psi, dtype=np.complex128)
+        h1 = np.zeros_like(psi) if h1 is None else h1
+        own = None if owned is None else np.ascontiguousarray(owned, dtype=np.uint8)
+        check(lib().tcg_apply_h1(self.handle, C.c_uint32(_terms(terms)), nb.ctypes.data_as(C.POINTER(C.c_int32)),
+                                 psi.ctypes.data, h1.ctypes.data, None if own is None else own.ctypes.data))
+        return h1
 
     def apply_device(self, terms, psi_ptr, h2_ptr, h3_ptr, nb_apply=None, owned=None):
         """Device-memory apply on the context's stream (pointers as ints)."""

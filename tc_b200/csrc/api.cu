@@ -11,6 +11,7 @@
 #include "passes.cuh"
 #include "util.cuh"
 #include "terms.cuh"
+#include "onebody.cuh"
 
 namespace tcg {
 
@@ -47,6 +48,103 @@ static int validate_system(const tcg_system_desc *s)
     if (!(s->omega > 0)) return fail(TCG_ERR_ARG, "unit-cell volume must be positive");
     if (s->includes_div_correction && !s->sum_Vaux) return fail(TCG_ERR_ARG, "sum_Vaux required with div correction");
     if (s->nsymop < 0) return fail(TCG_ERR_ARG, "negative nsymop");
+    return TCG_OK;
+}
+
+// Pencil table of the pruned transforms (36^3 path).  A pair density
+// conj(a_q(r)) b_k(r) of two orbitals on the plane-wave spheres of q and k
+// has Fourier components G = G1 - G2 with |k + G1| <= R_k and |q + G2| <= R_q,
+// so it vanishes outside the ball |G + k - q| < R_k + R_q; for every
+// (irreducible k, all-k q) pair the table marks the (x, y) pencils of the grid
+// that meet that ball, and lists them first.  Built only when no ball reaches
+// past the grid's Miller range (the support would wrap) and the table stays
+// under 256 MB.
+static int build_prune_table(tcg_ctx *c)
+{
+    Host &h = c->h;
+    c->prune_ok = false;
+    const int n0 = h.n[0], n1 = h.n[1], n2 = h.n[2], np = n0 * n1;
+    const size_t nent = (size_t)h.nk * h.nk_all;
+    if (nent * np * 3 + nent * sizeof(int) + nent * n0 * 8 > ((size_t)256 << 20)) return TCG_OK;
+    auto cartv = [&](const double *x, double *v) {
+        for (int d = 0; d < 3; d++) v[d] = h.recip[0 * 3 + d] * x[0] + h.recip[1 * 3 + d] * x[1] + h.recip[2 * 3 + d] * x[2];
+    };
+    auto signed_m = [](int i, int n) { return i <= n / 2 ? i : i - n; };
+    // sphere radius of every irreducible k: max |k + G| over its plane waves
+    std::vector<double> R(h.nk, 0.0);
+    for (int k = 0; k < h.nk; k++) {
+        double kc[3];
+        cartv(&h.kvec[3 * h.kall_off[k]], kc);
+        const size_t o = h.gidx_off[h.kall_off[k]];
+        for (int p = 0; p < h.npw[k]; p++) {
+            const int gi = h.gidx_host[o + p];
+            const double m[3] = {(double)signed_m(gi % n0, n0), (double)signed_m((gi / n0) % n1, n1),
+                                 (double)signed_m(gi / np, n2)};
+            double G[3];
+            cartv(m, G);
+            const double r = sqrt((kc[0] + G[0]) * (kc[0] + G[0]) + (kc[1] + G[1]) * (kc[1] + G[1]) +
+                                  (kc[2] + G[2]) * (kc[2] + G[2]));
+            R[k] = std::max(R[k], r);
+        }
+    }
+    // |a_i| / (2 pi): Miller extent of a Cartesian length
+    double alen[3];
+    for (int i = 0; i < 3; i++)
+        alen[i] = sqrt(h.lattice[3 * i] * h.lattice[3 * i] + h.lattice[3 * i + 1] * h.lattice[3 * i + 1] +
+                       h.lattice[3 * i + 2] * h.lattice[3 * i + 2]) / (2.0 * PI_D);
+    const double *b1 = &h.recip[0], *b2 = &h.recip[3], *b3 = &h.recip[6];
+    const double b33 = b3[0] * b3[0] + b3[1] * b3[1] + b3[2] * b3[2];
+    if (n1 > 64) return TCG_OK;                       // column bit masks hold 64 rows
+    const size_t bits_off = (nent * np * 3 + nent * sizeof(int) + 7) & ~(size_t)7;
+    std::vector<unsigned char> tab(bits_off + nent * n0 * sizeof(unsigned long long));
+    unsigned char *mask = tab.data();
+    unsigned short *perm = reinterpret_cast<unsigned short *>(tab.data() + nent * np);
+    int *nact = reinterpret_cast<int *>(tab.data() + nent * np * 3);
+    unsigned long long *bits = reinterpret_cast<unsigned long long *>(tab.data() + bits_off);
+    const int zlo = -((n2 - 1) / 2), zhi = n2 / 2;
+    for (int ik = 0; ik < h.nk; ik++)
+        for (int a = 0; a < h.nk_all; a++) {
+            const size_t e = (size_t)ik * h.nk_all + a;
+            double kk[3], qq[3], kq[3];
+            cartv(&h.kvec[3 * h.kall_off[ik]], kk);
+            cartv(&h.kvec[3 * a], qq);
+            for (int d = 0; d < 3; d++) kq[d] = kk[d] - qq[d];
+            const double Rr = (R[ik] + R[h.ik_of_all[a]]) * (1.0 + 1e-9) + 1e-9;
+            // the ball centre -kq in Miller coordinates: m_i = -kq . a_i / (2 pi)
+            for (int i = 0; i < 3; i++) {
+                const double ci = -(kq[0] * h.lattice[3 * i] + kq[1] * h.lattice[3 * i + 1] + kq[2] * h.lattice[3 * i + 2]) /
+                                  (2.0 * PI_D);
+                if (fabs(ci) + Rr * alen[i] >= (h.n[i] - 1) / 2.0) return TCG_OK;   // support could wrap
+            }
+            int na = 0;
+            std::vector<int> act, inact;
+            for (int y = 0; y < n1; y++)
+                for (int x = 0; x < n0; x++) {
+                    const int mx = signed_m(x, n0), my = signed_m(y, n1);
+                    double P[3];
+                    for (int d = 0; d < 3; d++) P[d] = mx * b1[d] + my * b2[d] + kq[d];
+                    const double bb = P[0] * b3[0] + P[1] * b3[1] + P[2] * b3[2];
+                    const double cc = P[0] * P[0] + P[1] * P[1] + P[2] * P[2] - Rr * Rr;
+                    const double disc = bb * bb - b33 * cc;
+                    bool on = false;
+                    if (disc >= 0) {
+                        const double lo = (-bb - sqrt(disc)) / b33 - 1e-9, hi = (-bb + sqrt(disc)) / b33 + 1e-9;
+                        const double zl = std::max(ceil(lo), (double)zlo), zh = std::min(floor(hi), (double)zhi);
+                        on = zl <= zh;
+                    }
+                    mask[e * np + x + n0 * y] = on ? 1 : 0;
+                    if (on) bits[e * n0 + x] |= 1ull << y;
+                    (on ? act : inact).push_back(x + n0 * y);
+                    na += on;
+                }
+            for (size_t i = 0; i < act.size(); i++) perm[e * np + i] = (unsigned short)act[i];
+            for (size_t i = 0; i < inact.size(); i++) perm[e * np + act.size() + i] = (unsigned short)inact[i];
+            nact[e] = na;
+        }
+    TRY(up(c->prune_tab, tab.data(), tab.size(), c->stream));
+    TCG_CUDA(cudaStreamSynchronize(c->stream));
+    c->prune_nact.assign(nact, nact + nent);
+    c->prune_ok = true;
     return TCG_OK;
 }
 
@@ -132,6 +230,7 @@ extern "C" int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg
             off += h.npw[h.ik_of_all[a]];
         }
     const size_t ngi = off;
+    h.gidx_host.assign(sys->gindex, sys->gindex + ngi);
     std::vector<int> inv((size_t)h.nspin * h.nk_all * h.N, -1);
     for (int s = 0; s < h.nspin && rc == TCG_OK; s++)
         for (int a = 0; a < h.nk_all && rc == TCG_OK; a++) {
@@ -145,6 +244,15 @@ extern "C" int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg
             }
         }
     if (rc != TCG_OK) { delete c; return rc; }
+    // plane-wave -> grid index of every (spin, irreducible k) at isym 0 (one-body terms)
+    std::vector<int> g0;
+    h.g0_off.resize((size_t)h.nspin * h.nk);
+    for (int s = 0; s < h.nspin; s++)
+        for (int k = 0; k < h.nk; k++) {
+            h.g0_off[(size_t)s * h.nk + k] = g0.size();
+            const size_t o = h.gidx_off[(size_t)s * h.nk_all + h.kall_off[k]];
+            g0.insert(g0.end(), sys->gindex + o, sys->gindex + o + h.npw[k]);
+        }
     // FFT plans
     GridDesc &g = c->gd;
     g.n0 = h.n[0]; g.n1 = h.n[1]; g.n2 = h.n[2]; g.N = h.N;
@@ -170,7 +278,8 @@ extern "C" int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg
             (rc = up(c->tw32, t32.data(), t32.size() * sizeof(float2), c->stream)) ||
             (rc = up(c->recip, h.recip, sizeof h.recip, c->stream)) ||
             (rc = up(c->inv, inv.data(), inv.size() * sizeof(int), c->stream)) ||
-            (rc = up(c->phase, sys->phase, ngi * sizeof(double2), c->stream))) {
+            (rc = up(c->phase, sys->phase, ngi * sizeof(double2), c->stream)) ||
+            (rc = up(c->gidx0, g0.data(), g0.size() * sizeof(int), c->stream))) {
             tcg_ctx_destroy(c);
             return rc;
         }
@@ -187,6 +296,12 @@ extern "C" int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg
             if (h.n[0] == f) c->fast_n = f;
     }
     if (getenv("TCG_GENERIC_PASSES")) c->force_generic = true;
+    if (getenv("TCG_NO_PRUNE")) c->no_prune = true;
+    if (getenv("TCG_SACC")) c->use_sacc = true;
+    if (c->fast_n == 36 && (rc = build_prune_table(c)) != TCG_OK) {
+        tcg_ctx_destroy(c);
+        return rc;
+    }
     if (const char *e = getenv("TCG_XY_KERNELS"))   // "line" / "pair": override the per-term choice
         c->xy_kernels = !strcmp(e, "line") ? 1 : (!strcmp(e, "pair") ? 2 : (!strcmp(e, "t6") ? 3 : 0));
     if (getenv("TCG_NO_PREFETCH")) c->no_prefetch = true;
@@ -201,7 +316,8 @@ extern "C" int tcg_ctx_destroy(tcg_ctx *c)
 {
     if (!c) return TCG_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    DBuf *bufs[] = {&c->tw64, &c->tw32, &c->recip, &c->inv, &c->phase, &c->phik, &c->chik, &c->fill,
+    DBuf *bufs[] = {&c->gpsi, &c->adjw, &c->adjt, &c->prune_tab, &c->VH, &c->V2h, &c->pgw, &c->gidx0, &c->vloc, &c->nlB, &c->nlD, &c->acc1, &c->h1buf,
+                    &c->tw64, &c->tw32, &c->recip, &c->inv, &c->phase, &c->phik, &c->chik, &c->fill,
                     &c->Rocc, &c->Rchi, &c->Rgrad, &c->dens, &c->densT, &c->occfill, &c->Vloc, &c->dnu, &c->dnuT,
                     &c->V3a1, &c->V3b1, &c->V3a2, &c->V3b2, &c->Qt, &c->Bt, &c->accP, &c->qtg, &c->div3b6,
                     &c->psi, &c->h2, &c->h3, &c->Rpsi, &c->Rgpsi, &c->acc2, &c->acc3, &c->qsum, &c->tmp,
@@ -307,9 +423,9 @@ static int check_apply(tcg_ctx *c, uint32_t mask, const int32_t *nb)
     if (!c || !nb) return fail(TCG_ERR_ARG, "null argument");
     if (!c->h.have_state) return fail(TCG_ERR_STATE, "tcg_set_state must be called before tcg_apply");
     const bool hf = c->h.method == TCG_METHOD_HF;
-    if (mask & ~(TCG_TERMS_HF | TCG_TERMS_TC)) return fail(TCG_ERR_ARG, "unknown term bits");
-    if (hf && (mask & ~TCG_TERMS_HF)) return fail(TCG_ERR_ARG, "TC terms requested for an HF context");
-    if (!hf && (mask & TCG_TERM_HF2X)) return fail(TCG_ERR_ARG, "hf2x requested for a TC/BITC context");
+    if (mask & ~(TCG_TERMS_H2 | TCG_TERMS_TC)) return fail(TCG_ERR_ARG, "unknown term bits (one-body terms: tcg_apply_h1)");
+    if (hf && (mask & ~(TCG_TERM_HF2X | TCG_TERM_HF2H))) return fail(TCG_ERR_ARG, "TC terms requested for an HF context");
+    if (!hf && (mask & (TCG_TERM_HF2X | TCG_TERM_HF2H))) return fail(TCG_ERR_ARG, "HF terms requested for a TC/BITC context");
     for (int i = 0; i < c->h.nspin * c->h.nk; i++)
         if (nb[i] < 0) return fail(TCG_ERR_ARG, "negative band count");
     return TCG_OK;
@@ -328,8 +444,8 @@ extern "C" int tcg_apply_device(tcg_ctx *c, uint32_t mask, const int32_t *nb, co
 {
     TRY(check_apply(c, mask, nb));
     if (!psi) return fail(TCG_ERR_ARG, "psi is NULL");
-    if ((mask & (TCG_TERM_HF2X | TCG_TERM_TC2X)) && !h2) return fail(TCG_ERR_ARG, "h2 is NULL");
-    if ((mask & ~(TCG_TERM_HF2X | TCG_TERM_TC2X)) && !h3) return fail(TCG_ERR_ARG, "h3 is NULL");
+    if ((mask & TCG_TERMS_H2) && !h2) return fail(TCG_ERR_ARG, "h2 is NULL");
+    if ((mask & ~TCG_TERMS_H2) && !h3) return fail(TCG_ERR_ARG, "h3 is NULL");
     ApplyArgs A{};
     A.mask = mask;
     A.nb = nb;
@@ -345,8 +461,8 @@ extern "C" int tcg_apply(tcg_ctx *c, uint32_t mask, const int32_t *nb, const dou
 {
     TRY(check_apply(c, mask, nb));
     if (!psi) return fail(TCG_ERR_ARG, "psi is NULL");
-    const bool need2 = mask & (TCG_TERM_HF2X | TCG_TERM_TC2X);
-    const bool need3 = mask & ~(TCG_TERM_HF2X | TCG_TERM_TC2X);
+    const bool need2 = mask & TCG_TERMS_H2;
+    const bool need3 = mask & ~TCG_TERMS_H2;
     if (need2 && !h2) return fail(TCG_ERR_ARG, "h2 is NULL");
     if (need3 && !h3) return fail(TCG_ERR_ARG, "h3 is NULL");
     const size_t n = psi_count(c, nb);
@@ -390,6 +506,36 @@ extern "C" int tcg_qp_finish(tcg_ctx *c)
     if (!h.qp_pending) return fail(TCG_ERR_STATE, "tcg_qp_finish without a pending tcg_qp_partial");
     h.qp_pending = false;
     return c->prec == TCG_PREC_FP64 ? qp_finish<double>(c) : qp_finish<float>(c);
+}
+
+extern "C" int tcg_set_pseudo(tcg_ctx *c, const tcg_pseudo_desc *pp)
+{
+    if (!c) return fail(TCG_ERR_ARG, "null context");
+    c->h.have_pseudo = false;
+    return set_pseudo(c, pp);
+}
+
+extern "C" int tcg_apply_h1(tcg_ctx *c, uint32_t mask, const int32_t *nb, const double *psi, double *h1,
+                            const uint8_t *owned)
+{
+    if (!c || !nb || !psi || !h1) return fail(TCG_ERR_ARG, "null argument");
+    if (mask & ~TCG_TERMS_H1) return fail(TCG_ERR_ARG, "tcg_apply_h1 applies the one-body terms only");
+    if ((mask & TCG_TERM_PSEUDO) && !c->h.have_pseudo) return fail(TCG_ERR_STATE, "tcg_set_pseudo must come first");
+    for (int i = 0; i < c->h.nspin * c->h.nk; i++)
+        if (nb[i] < 0) return fail(TCG_ERR_ARG, "negative band count");
+    const size_t n = psi_count(c, nb);
+    for (size_t i = 0; i < 2 * n; i++)
+        if (!std::isfinite(psi[i])) return fail(TCG_ERR_NUMERIC, "non-finite value in psi");
+    const size_t bytes = n * sizeof(double2);
+    TRY(c->psi.ensure(std::max<size_t>(16, bytes)));
+    TRY(c->h1buf.ensure(std::max<size_t>(16, bytes)));
+    TCG_CUDA(cudaMemcpyAsync(c->psi.p, psi, bytes, cudaMemcpyHostToDevice, c->stream));
+    TCG_CUDA(cudaMemcpyAsync(c->h1buf.p, h1, bytes, cudaMemcpyHostToDevice, c->stream));
+    TRY(c->prec == TCG_PREC_FP64 ? apply_h1_impl<double>(c, mask, nb, c->psi.as<double2>(), c->h1buf.as<double2>(), owned)
+                                 : apply_h1_impl<float>(c, mask, nb, c->psi.as<double2>(), c->h1buf.as<double2>(), owned));
+    TCG_CUDA(cudaMemcpyAsync(h1, c->h1buf.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    TCG_CUDA(cudaStreamSynchronize(c->stream));
+    return TCG_OK;
 }
 
 extern "C" int tcg_set_tuning(tcg_ctx *c, int64_t tmp_budget_bytes)
@@ -698,6 +844,26 @@ extern "C" int tcg_energy(tcg_ctx *c, const int32_t *nb, const void *h2_dev, con
     TCG_CUDA(cudaMemcpyAsync(e_out, base + b3, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     TCG_CUDA(cudaStreamSynchronize(c->stream));
     return TCG_OK;
+}
+
+#include "adjoint.cuh"
+
+extern "C" int tcg_energy_grad(tcg_ctx *c, uint32_t mask, double *e_out, void *dchi, double *du, double *dv2)
+{
+    if (!c || !e_out) return fail(TCG_ERR_ARG, "null argument");
+    Host &h = c->h;
+    if (!h.have_state) return fail(TCG_ERR_STATE, "tcg_set_state must be called before tcg_energy_grad");
+    TRY(check_apply(c, mask, std::vector<int32_t>((size_t)h.nspin * h.nk, 0).data()));
+    if (dchi)
+        for (int k = 0; k < h.nk; k++)
+            if (h.nsym_k[k] != 1)
+                return fail(TCG_ERR_UNSUPPORTED, "orbital gradient needs every k-point irreducible alone (nsym_k = 1)");
+    if (du || dv2) {
+        if (h.nk_all != 1) return fail(TCG_ERR_UNSUPPORTED, "Jastrow-table gradients are implemented for Gamma-only systems");
+        if (!(mask & TCG_TERM_TC2X)) return fail(TCG_ERR_ARG, "Jastrow-table gradients need TCG_TERM_TC2X in the mask");
+    }
+    return c->prec == TCG_PREC_FP64 ? energy_grad_impl<double>(c, mask, e_out, dchi, du, dv2)
+                                    : energy_grad_impl<float>(c, mask, e_out, dchi, du, dv2);
 }
 
 // ------------------------------------------------------------- profiling --

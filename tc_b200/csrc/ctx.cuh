@@ -69,6 +69,7 @@ struct Host {
     std::vector<int> rotation;              // [nsymop][9]
     std::vector<double> translation;        // [nsymop][3]
     std::vector<size_t> gidx_off;           // [nspin*nk_all] offset in gindex / phase
+    std::vector<int> gidx_host;             // host copy of gindex (pseudopotential set-up)
     double A[4], F[4];
     bool A_zero = true;
     bool div = false;
@@ -83,6 +84,12 @@ struct Host {
     size_t nocc_grids = 0;
     bool qp_ready = false;                  // tc3a2a4b2b5 occupied-pair stage done for this state
     bool qp_pending = false;                // a partial stage awaits the caller's sum and tcg_qp_finish
+    // one-body data
+    bool have_pseudo = false, have_vloc = false;
+    int nl_ncomp = 0;                       // projector components (atom, projector, m)
+    std::vector<size_t> nl_koff;            // [nk] offset of k in nlB
+    size_t nl_dval_off = 0;                 // byte offset of the D values in nlD
+    std::vector<size_t> g0_off;             // [nspin*nk] offset of (s, k) in gidx0
 };
 
 struct tcg_ctx_impl;
@@ -109,6 +116,23 @@ struct tcg_ctx {
     tcg::DBuf Vloc;                         // [nspin][N] double2 (tc3a1 + tc3b1 + ...)
     tcg::DBuf dnu, dnuT;                    // [nspin][3][N] fp64 / compute precision
     tcg::DBuf V3a1, V3b1, V3a2, V3b2;       // [nspin][N] fp64 local three-body potentials
+    tcg::DBuf VH;                           // [N] fp64 Hartree potential (hf2h)
+    tcg::DBuf V2h;                          // [nspin][N] fp64 TC Hartree potential (tc2h [2a_h] + [2b_h2])
+    tcg::DBuf pgw;                          // [3][N] fp64 work: sum_q f conj(chi_q) grad phi_q (tc2h [2b_h2])
+    // one-body data (tcg_set_pseudo) and per-apply scratch
+    tcg::DBuf gidx0;                        // [nspin][sum npw] grid index of each plane wave at isym 0
+    tcg::DBuf vloc;                         // [N] fp64 local pseudopotential (real), or empty
+    tcg::DBuf nlB;                          // [sum_k ncomp npw_k] complex exp(iG.R) x projector
+    tcg::DBuf nlD;                          // CSR of D between projector components
+    tcg::DBuf acc1, h1buf;                  // one-body accumulators / device copies
+    tcg::DBuf gpsi, adjw, adjt;             // energy gradients: occupied block + outputs, pair grids, tables
+    // pruned transforms (36^3 path): per (irreducible k, all-k q) pair, the
+    // (x, y) pencils of the grid that the support of a pair density touches
+    tcg::DBuf prune_tab;                    // masks [nk][nk_all][NP] u8, perms [..][NP] u16, counts [..] i32
+    bool prune_ok = false;                  // table built and usable
+    std::vector<int> prune_nact;            // host copy of the table's active-pencil counts
+    bool no_prune = false;                  // TCG_NO_PRUNE: full transforms everywhere
+    bool use_sacc = false;                  // TCG_SACC: shared-memory accumulation in the 3a3b6A inverse XY pass
     tcg::DBuf Qt, Bt;                       // tc3a2a4b2b5 rotated intermediates [nocc_grids][3][N]
     tcg::DBuf accP, qtg;                    // occupied-pair accumulators / gathered q2 grids
     tcg::DBuf div3b6;                       // [nspin][N] fp64 temp_div_3b6 in R space

@@ -183,8 +183,16 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 3)
         if (pid < nplanes) {
             const int item = pid / N, z = pid % N;
             V *dst = op.tmp_grid(item, f) + (size_t)z * N * N + ln;
+            if (((Op::BLI >> f) & 1) && op.m.prune) {
+                // band-limited input: only the pencils its support meets are read by the Z pass
+                const unsigned long long bits = op.pcol(item, ln);
 #pragma unroll
-            for (int i = 0; i < N; i++) dst[i * N] = v[i];
+                for (int i = 0; i < N; i++)
+                    if ((bits >> i) & 1) dst[i * N] = v[i];
+            } else {
+#pragma unroll
+                for (int i = 0; i < N; i++) dst[i * N] = v[i];
+            }
         }
     }
 }
@@ -690,8 +698,15 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyf_t6(Op op, int nplanes)
         xform<V, -1, true>(A + l * PAD, 1, t, tw, v);      // rows
         xform<V, -1, false>(A + l, PAD, t, tw, v);         // columns: v[k2] at y = t + 6 k2
         V *dst = op.tmp_grid(item, f) + pz + l;
+        if (((Op::BLI >> f) & 1) && op.m.prune) {
+            const unsigned long long bits = op.pcol(item, l);
 #pragma unroll
-        for (int k2 = 0; k2 < R; k2++) dst[(size_t)(t + R * k2) * N] = v[k2];
+            for (int k2 = 0; k2 < R; k2++)
+                if ((bits >> (t + R * k2)) & 1) dst[(size_t)(t + R * k2) * N] = v[k2];
+        } else {
+#pragma unroll
+            for (int k2 = 0; k2 < R; k2++) dst[(size_t)(t + R * k2) * N] = v[k2];
+        }
     }
 }
 
@@ -714,17 +729,45 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
     const size_t pz = (size_t)z * N * N;
     const int ns = op.nsrc(tj);
     constexpr bool RACC = Op::REGACC && sizeof(V) == 8;
+    constexpr int SA = sizeof(V) == 8 ? Op::SACC : 0;    // shared-memory accumulator planes (FP32)
+    const bool sa_on = SA > 0 && op.sacc_on;
     static_assert(!(RACC && Op::REFWD), "re-forwarded outputs accumulate through xyi_accum");
     static_assert(!(Op::REFWD && Op::GS > 1), "re-forward needs GS == 1");
+    static_assert(!(SA > 0 && (RACC || Op::GS > 1)), "shared-memory accumulation replaces the other forms");
     V racc[R], keep[Op::GS][R];
 #pragma unroll
     for (int i = 0; i < R; i++) racc[i] = czero<V>();
+    V *SAcc = W + 2 * PS;                 // [SA][N][N]: this thread owns y = t + 6 k2, x = l
+    // pruned chunks: the pencil-table entry of every source, looked up once
+    // (the copies of each step then need one load of their column mask)
+    int *sent = reinterpret_cast<int *>(SAcc + (sa_on ? SA * N * N : 0));
+    if (op.m.prune) {
+        for (int si = threadIdx.x; si < ns; si += blockDim.x) sent[si] = op.pent_of(op.item_of(tj, si));
+        __syncthreads();
+    }
+    if (sa_on) {
+#pragma unroll
+        for (int a = 0; a < SA; a++)
+#pragma unroll
+            for (int k2 = 0; k2 < R; k2++) SAcc[(a * N + t + R * k2) * N + l] = czero<V>();
+    }
     const int total = ns * Op::NB;        // it = si * NB + b
     auto issue = [&](int it) {
-        const V *src = op.xyi_grid(op.item_of(tj, it / Op::NB), it % Op::NB) + pz + l;
+        const int item = op.item_of(tj, it / Op::NB), b = it % Op::NB;
+        const V *src = op.xyi_grid(item, b) + pz + l;
         V *dst = W + (it & 1) * PS + l;
+        if (((Op::BLO >> b) & 1) && op.m.prune) {
+            // band-limited output: the Z pass wrote only the pencils its support meets
+            const unsigned long long bits = op.m.pbits[(size_t)sent[it / Op::NB] * op.g.n0 + l];
 #pragma unroll
-        for (int m = 0; m < R; m++) cp_async_elem(dst + (t + R * m) * PAD, src + (size_t)(t + R * m) * N);
+            for (int m = 0; m < R; m++) {
+                if ((bits >> (t + R * m)) & 1) cp_async_elem(dst + (t + R * m) * PAD, src + (size_t)(t + R * m) * N);
+                else dst[(t + R * m) * PAD] = czero<V>();
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < R; m++) cp_async_elem(dst + (t + R * m) * PAD, src + (size_t)(t + R * m) * N);
+        }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
     issue(0);
@@ -748,7 +791,16 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
             continue;
         }
         const int item = op.item_of(tj, si);
-        if (RACC && op.regacc_grid(b0)) {
+        if (sa_on) {
+            const int slot = op.xyi_slot(b0);      // uniform over the CTA
+            if (slot >= 0) {
+#pragma unroll
+                for (int k2 = 0; k2 < R; k2++) {
+                    V *a = &SAcc[(slot * N + t + R * k2) * N + l];
+                    *a = cadd(*a, op.xyi_sterm(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, v[k2]));
+                }
+            }
+        } else if (RACC && op.regacc_grid(b0)) {
 #pragma unroll
             for (int k2 = 0; k2 < R; k2++) {
                 V vals[1] = {v[k2]};
@@ -784,6 +836,17 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
 #pragma unroll
         for (int k2 = 0; k2 < R; k2++) op.xyi_flush(tj, pz + (size_t)(t + R * k2) * N + l, racc[k2]);
     }
+    if (sa_on) {
+#pragma unroll
+        for (int a = 0; a < SA; a++)
+#pragma unroll
+            for (int k2 = 0; k2 < R; k2++)
+                op.xyi_sflush(tj, a, pz + (size_t)(t + R * k2) * N + l, SAcc[(a * N + t + R * k2) * N + l]);
+    }
+}
+template <typename V, class Op> __host__ inline size_t smem_xyi(int sets, bool sacc_on)
+{
+    return sizeof(V) * (128 + (size_t)sets * N * PAD + (sizeof(V) == 8 && sacc_on ? (size_t)Op::SACC * N * N : 0));
 }
 
 // Z pass: one item and 32 consecutive pencils (x, y) per CTA, six threads
@@ -803,23 +866,41 @@ __global__ void __launch_bounds__(ZTHREADS, 4) k_z_t6(Op op)
     const Tw<V> tw = stage<V>(op.g, tws);
     const int item = blockIdx.y;
     const int t = threadIdx.x / TC, cl = threadIdx.x % TC;
-    const int c = blockIdx.x * TC + cl;
-    const bool act = c < N * N;
+    // pruning: the CTA takes its 32 pencils from the pair's list (active
+    // pencils first); a CTA past the active ones skips the band-limited
+    // inputs (zero) and outputs (never read)
+    const bool prune = op.m.prune != 0;
+    const int slot = blockIdx.x * TC + cl;
+    int c = slot;
+    bool allin = false, pon = true;
+    if (prune) {
+        const int e = op.pent_of(item);
+        allin = blockIdx.x * TC >= op.m.pnact[e];
+        if (slot < N * N) {
+            c = op.m.pperm[(size_t)e * op.m.np + slot];
+            pon = slot < op.m.pnact[e];
+        }
+    }
+    const bool act = slot < N * N;
     const int x = c % N, y = c / N;
 #pragma unroll
     for (int f = 0; f < Op::NF; f++) {
+        const bool bl = prune && ((Op::BLI >> f) & 1);
         const V *src = op.zin_grid(item, f) + c;
 #pragma unroll
         for (int m = 0; m < R; m++) {
             const int z = t + R * m;
-            S[(f * N + z) * TC + cl] = act ? src[(size_t)z * N * N] : czero<V>();
+            S[(f * N + z) * TC + cl] = (act && (!bl || pon)) ? src[(size_t)z * N * N] : czero<V>();
         }
     }
     __syncthreads();
     V v[R];
 #pragma unroll
-    for (int f = 0; f < Op::NF; f++) xform<V, -1, true>(S + f * N * TC + cl, TC, t, tw, v);
+    for (int f = 0; f < Op::NF; f++)
+        if (!(allin && ((Op::BLI >> f) & 1))) xform<V, -1, true>(S + f * N * TC + cl, TC, t, tw, v);
     for (int o = 0; o < Op::NB; o++) {
+        const bool blo = prune && ((Op::BLO >> o) & 1);
+        if (blo && allin) continue;       // uniform over the CTA
         if (Op::ZINV) __syncthreads();    // the previous output's sweep has read O
 #pragma unroll
         for (int m = 0; m < R; m++) {
@@ -834,7 +915,7 @@ __global__ void __launch_bounds__(ZTHREADS, 4) k_z_t6(Op op)
         if (Op::ZINV) {
             __syncthreads();
             xform<V, +1, false>(O + cl, TC, t, tw, v);   // v[k2] at z = t + 6 k2
-            if (act) {
+            if (act && (!blo || pon)) {
                 V *dst = op.out_grid(item, o) + c;
 #pragma unroll
                 for (int k2 = 0; k2 < R; k2++) dst[(size_t)(t + R * k2) * N * N] = v[k2];
@@ -861,15 +942,28 @@ __global__ void __launch_bounds__(ZTHREADS, 3) k_z_t6r(Op op)
     const Tw<V> tw = stage<V>(op.g, tws);
     const int item = blockIdx.y;
     const int t = threadIdx.x / TC, cl = threadIdx.x % TC;
-    const int c = blockIdx.x * TC + cl;
-    const bool act = c < N * N;
+    // pruning as in k_z_t6 (band-limited inputs read as zero off their support)
+    const bool prune = op.m.prune != 0;
+    const int slot = blockIdx.x * TC + cl;
+    int c = slot;
+    bool allin = false, pon = true;
+    if (prune) {
+        const int e = op.pent_of(item);
+        allin = blockIdx.x * TC >= op.m.pnact[e];
+        if (slot < N * N) {
+            c = op.m.pperm[(size_t)e * op.m.np + slot];
+            pon = slot < op.m.pnact[e];
+        }
+    }
+    const bool act = slot < N * N;
     const int x = c % N, y = c / N;
     V X[NF][R];
 #pragma unroll
     for (int f = 0; f < NF; f++) {
+        const bool bl = prune && ((Op::BLI >> f) & 1);
         const V *src = op.zin_grid(item, f) + c;
 #pragma unroll
-        for (int m = 0; m < R; m++) X[f][m] = act ? src[(size_t)(t + R * m) * N * N] : czero<V>();
+        for (int m = 0; m < R; m++) X[f][m] = (act && (!bl || pon)) ? src[(size_t)(t + R * m) * N * N] : czero<V>();
     }
 #pragma unroll
     for (int f = 0; f < NF; f++) {
@@ -889,6 +983,8 @@ __global__ void __launch_bounds__(ZTHREADS, 3) k_z_t6r(Op op)
         line_fft<V, R, -1>(X[f], tw.w6);   // X[f][k2]: input f at z = t + 6 k2
     }
     for (int o = 0; o < Op::NB; o++) {
+        const bool blo = prune && ((Op::BLO >> o) & 1);
+        if (blo && allin) continue;       // uniform over the CTA
         V v[R];
 #pragma unroll
         for (int k2 = 0; k2 < R; k2++) {
@@ -912,7 +1008,7 @@ __global__ void __launch_bounds__(ZTHREADS, 3) k_z_t6r(Op op)
             for (int j = 0; j < R; j++) v[j] = E[(t * R + j) * TC + cl];
             line_fft<V, R, +1>(v, tw.w6);     // v[k2] at z = t + 6 k2
         }
-        if (act) {
+        if (act && (!blo || pon)) {
             V *dst = op.out_grid(item, o) + c;
 #pragma unroll
             for (int k2 = 0; k2 < R; k2++) dst[(size_t)(t + R * k2) * N * N] = v[k2];

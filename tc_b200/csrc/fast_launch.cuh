@@ -12,6 +12,11 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
     using V = typename C2<T>::t;
     using CF = fast::Cfg<N, sizeof(V)>;
     const double gb = (double)N * N * N * sizeof(V);
+    // bytes a pass must move: N s per grid, the band-limited grids of a pruned
+    // chunk only on the pencils their support meets (fraction op.m.pfrac)
+    const double fr = op.m.prune ? op.m.pfrac : 1.0;
+    const int bli = __builtin_popcount(Op::BLI), blo = __builtin_popcount(Op::BLO);
+    const double nf_eff = (Op::NF - bli) + fr * bli, nb_eff = (Op::NB - blo) + fr * blo;
     const int np_f = items * N, np_i = nt * N;
     using CP = fast::CfgP<N, sizeof(V)>;
     const bool fpair = c->xy_kernels ? c->xy_kernels == 2 : Op::XYF_PAIR;
@@ -23,12 +28,12 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
     const bool t6f = N == 36 && (c->xy_kernels == 3 || (c->xy_kernels == 0 && sizeof(V) == 16));
     if constexpr (N == 36) {
         if (t6f && do_xyf)
-            TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * Op::NF * gb, fast::t6::k_xyf_t6<T, Op>,
+            TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * nf_eff * gb, fast::t6::k_xyf_t6<T, Op>,
                               dim3(np_f), dim3(fast::t6::THREADS), fast::t6::smem<V>(1), op, np_f));
     }
     if (do_xyf && !t6f) {
         if (!fpair)
-            TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * Op::NF * gb, fast::k_xyf_fast<T, N, Op>,
+            TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * nf_eff * gb, fast::k_xyf_fast<T, N, Op>,
                               dim3((np_f + CF::P - 1) / CF::P), dim3(CF::THREADS), fast::smem_xy_fast<V, N>(1), op, np_f));
         else
             TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * Op::NF * gb, fast::k_xyf_pair<T, N, Op>,
@@ -43,11 +48,11 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
         // default: inputs transformed in place in shared memory (k_z_t6); the
         // terms with Op::ZREG keep them in registers in FP32 (k_z_t6r)
         if (c->z_kernels == 3 || (c->z_kernels == 0 && !(Op::ZREG && sizeof(V) == 8)))
-            TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb,
+            TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (nf_eff + (Op::ZINV ? nb_eff : 0)) * gb,
                               fast::t6::k_z_t6<T, Op>, dim3((N * N + TC - 1) / TC, items), dim3(fast::t6::ZTHREADS),
                               fast::t6::smem_z<V>(Op::NF), op));
         else if (zt6)
-            TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb,
+            TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (nf_eff + (Op::ZINV ? nb_eff : 0)) * gb,
                               fast::t6::k_z_t6r<T, Op>, dim3((N * N + TC - 1) / TC, items), dim3(fast::t6::ZTHREADS),
                               fast::t6::smem_zr<V>(Op::NF), op));
     }
@@ -63,8 +68,10 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
     if constexpr (N == 36) {
         if (t6i && do_xyi) {
             const int nref = Op::REFWD ? Op::NB - 1 : 0;
-            return launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (Op::NB + nref) * gb,
-                                 fast::t6::k_xyi_t6<T, Op>, dim3(np_i), dim3(fast::t6::THREADS), fast::t6::smem<V>(2),
+            return launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (nb_eff + nref) * gb,
+                                 fast::t6::k_xyi_t6<T, Op>, dim3(np_i), dim3(fast::t6::THREADS),
+                                 fast::t6::smem_xyi<V, Op>(2, op.sacc_on != 0) +
+                                     (op.m.prune ? (size_t)op.ns * sizeof(int) : 0),
                                  op, np_i);
         }
     }

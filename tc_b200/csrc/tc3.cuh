@@ -326,12 +326,96 @@ __global__ void k_div3a2(GridDesc g, RecipC rc, Jastrow J, int sq, int nspin, in
     }
 }
 
+// ------------------------------------------------ Hartree-type two-body --
+// V_H(G) = 4 pi n(G) / |G|^2 with V_H(0) = 0, in place on n_0 + n_1 in G
+// (calc_hamiltonian_hf2h.cpp:40-50)
+static __global__ void k_hartree_g(GridDesc g, RecipC rc, double2 *V)
+{
+    const double zero[3] = {0, 0, 0};
+    const double FOURPI = 4.0 * 3.14159265358979323846;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += gridDim.x * blockDim.x) {
+        if (p == 0) { V[0] = {0, 0}; continue; }
+        int x, y, z;
+        xyz_of(g, p, x, y, z);
+        double G[3];
+        gvec(rc.R, g, x, y, z, zero, G);
+        const double f = FOURPI / (G[0] * G[0] + G[1] * G[1] + G[2] * G[2]);
+        V[p] = {V[p].x * f, V[p].y * f};
+    }
+}
+
+// tc2h [2b_h2]: out_d(r) = sum over the occupied grids of one spin of
+// f conj(chi(r)) grad_d phi(r), grids in order (calc_hamiltonian_tc2h.cpp:53-136)
+template <typename T>
+__global__ void k_phiq_gphiq(int N, int ngrid, const typename C2<T>::t *chi, const typename C2<T>::t *grad,
+                             const double *fill, double2 *out)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        double2 a[3] = {{0, 0}, {0, 0}, {0, 0}};
+        for (int gi = 0; gi < ngrid; gi++) {
+            const double2 c = to64(chi[(size_t)gi * N + p]);
+            const double f = fill[gi];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const double2 v = cmulc(c, to64(grad[((size_t)gi * 3 + d) * N + p]));
+                a[d] = {a[d].x + f * v.x, a[d].y + f * v.y};
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 3; d++) out[(size_t)d * N + p] = a[d];
+    }
+}
+
+// tc2h potential of spin s in G (calc_hamiltonian_tc2h.cpp:146-180):
+// V(G) = sum_js [ V_2body(G; s, js) n_js(G) + u(G; s, js) G . pg[js'](G) / spin_factor ]
+static __global__ void k_tc2h_g(GridDesc g, RecipC rc, Jastrow J, int s, int nspin, const double2 *nG,
+                                const double2 *pg, double2 *V)
+{
+    const double zero[3] = {0, 0, 0};
+    const double spin_factor = nspin == 1 ? 2.0 : 1.0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.N; p += gridDim.x * blockDim.x) {
+        int x, y, z;
+        xyz_of(g, p, x, y, z);
+        double G[3];
+        gvec(rc.R, g, x, y, z, zero, G);
+        double2 acc = {0, 0};
+        for (int js = 0; js < 2; js++) {
+            const int jr = nspin == 1 ? 0 : js;
+            const double2 n = nG[(size_t)js * g.N + p];
+            const double v2 = J.tc2body(G, s, js), u = J.uk(G, s, js);
+            acc = {acc.x + v2 * n.x, acc.y + v2 * n.y};
+            for (int d = 0; d < 3; d++) {
+                const double2 q = pg[((size_t)jr * 3 + d) * g.N + p];
+                acc = {acc.x + u * G[d] * q.x / spin_factor, acc.y + u * G[d] * q.y / spin_factor};
+            }
+        }
+        V[p] = acc;
+    }
+}
+
+// acc[t] += a (V(r) phi_t(r) - sum_d grad_d phi_t(r) W_d(r))   (tc2h.cpp:211-222;
+// hf2h.cpp:70-73 with W absent)
+template <typename T>
+__global__ void k_local_h2(int N, const typename C2<T>::t *Rpsi, const typename C2<T>::t *Rgpsi, const double2 *Vr,
+                           const double2 *W, double a, double2 *acc)
+{
+    const size_t t = blockIdx.y;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        double2 v = cmul(Vr[p], to64(Rpsi[t * N + p]));
+        if (W)
+            for (int d = 0; d < 3; d++) v = csub(v, cmul(to64(Rgpsi[(t * 3 + d) * N + p]), W[(size_t)d * N + p]));
+        acc_add(acc + t * N + p, v, a);
+    }
+}
+
 // ------------------------------------------------------- chunk planning --
 struct ChunkPlan {
     int t0, nt, s0, ns, nTB, nSB;
     size_t meta_off;         // byte offset in the meta arena
     const int *tb, *sb;
     const double *kq;
+    const int *pent;         // [nTB*nSB] pencil-table entry of each (target k, source q) pair
+    double pfrac;            // mean active-pencil fraction over the chunk's items
 };
 
 // Plan (target range x source range) chunks; kq = tcart[tkey] - scart[skey].
@@ -390,13 +474,26 @@ static int plan_chunks(tcg_ctx *c, DBuf &meta, int ntg, const std::vector<int> &
                 memcpy(host.data() + o, src, bytes);
                 return o;
             };
+            // pencil-table entry of each pair: target key (irreducible k) x source key (all-k)
+            std::vector<int> pent((size_t)p.nTB * p.nSB);
+            for (int a = 0; a < p.nTB; a++)
+                for (int b = 0; b < p.nSB; b++) pent[(size_t)a * p.nSB + b] = tk[a] * c->h.nk_all + sk[b];
+            p.pfrac = 1.0;
+            if (c->prune_ok) {
+                double sum = 0;
+                for (int i = 0; i < p.nt; i++)
+                    for (int j = 0; j < p.ns; j++) sum += c->prune_nact[pent[(size_t)tb[i] * p.nSB + sb[j]]];
+                p.pfrac = sum / ((double)p.nt * p.ns * c->h.n[0] * c->h.n[1]);
+            }
             p.meta_off = append(kq.data(), kq.size() * sizeof(double));
             size_t otb = append(tb.data(), tb.size() * sizeof(int));
             size_t osb = append(sb.data(), sb.size() * sizeof(int));
+            size_t ope = append(pent.data(), pent.size() * sizeof(int));
             // stash offsets in the pointer fields; resolved after upload
             p.kq = reinterpret_cast<const double *>(p.meta_off);
             p.tb = reinterpret_cast<const int *>(otb);
             p.sb = reinterpret_cast<const int *>(osb);
+            p.pent = reinterpret_cast<const int *>(ope);
             out.push_back(p);
         }
     TRY(meta.ensure(host.size() + 8));
@@ -406,6 +503,7 @@ static int plan_chunks(tcg_ctx *c, DBuf &meta, int ntg, const std::vector<int> &
         p.kq = reinterpret_cast<const double *>(base + (size_t)p.kq);
         p.tb = reinterpret_cast<const int *>(base + (size_t)p.tb);
         p.sb = reinterpret_cast<const int *>(base + (size_t)p.sb);
+        p.pent = reinterpret_cast<const int *>(base + (size_t)p.pent);
     }
     TCG_CUDA(cudaStreamSynchronize(c->stream));
     return TCG_OK;
@@ -491,6 +589,20 @@ static void op_common(tcg_ctx *c, Op &op, const ChunkPlan &p, int nsl, int ntab)
     op.m.nSB = p.nSB;
     op.m.ntab = ntab;
     op.m.nrec = c->ftab_nrec;
+    // pruning: 36^3 grid, default kernel forms (the kernels that honour it:
+    // k_xyf_fast / k_xyf_t6, k_z_t6 / k_z_t6r, k_xyi_t6), table built
+    const int np = c->h.n[0] * c->h.n[1];
+    op.m.np = np;
+    op.m.prune = (c->prune_ok && !c->no_prune && c->fast_n == 36 && !c->force_generic && c->xy_kernels == 0 &&
+                  c->z_kernels == 0 && (Op::BLI | Op::BLO) != 0) ? 1 : 0;
+    op.m.pent = p.pent;
+    op.m.pfrac = op.m.prune ? p.pfrac : 1.0;
+    const size_t nent = (size_t)c->h.nk * c->h.nk_all;
+    op.m.pmask = c->prune_tab.as<const unsigned char>();
+    op.m.pperm = reinterpret_cast<const unsigned short *>(c->prune_tab.as<const unsigned char>() + nent * np);
+    op.m.pnact = reinterpret_cast<const int *>(c->prune_tab.as<const unsigned char>() + nent * np * 3);
+    op.m.pbits = reinterpret_cast<const unsigned long long *>(
+        c->prune_tab.as<const unsigned char>() + ((nent * np * 3 + nent * sizeof(int) + 7) & ~(size_t)7));
     memcpy(op.rc.R, c->h.recip, sizeof op.rc.R);
     op.invN = 1.0 / (double)c->h.N;
 }
@@ -766,6 +878,7 @@ static int tc3_stage_ab(tcg_ctx *c, const Targets &Tg, const TRange &TR, const S
         a.tmp2 = c->tmp2.as<V>();
         a.s = s;
         a.b3 = b3;
+        a.sacc_on = c->use_sacc ? 1 : 0;
         TRY((run_chunk<T, OA>(c, a, (int)items, p.nt)));
         OB b;
         op_common<T>(c, b, p, nsl, 2);
@@ -1048,6 +1161,7 @@ static int qp_finish(tcg_ctx *c)
                 TCG_CUDA(cudaMemcpyAsync(c->aux.p, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
                 TRY(c->tmp.ensure((size_t)items * 2 * N * sizeof(V)));
                 OpPairFwd<T> op;
+                op.m = ChunkMeta{};
                 op.g = g;
                 op.tmp = c->tmp.as<V>();
                 op.nsl = 2;
@@ -1256,7 +1370,6 @@ static int state_terms(tcg_ctx *c)
     Host &h = c->h;
     h.qp_ready = false;
     h.qp_pending = false;
-    if (h.method == TCG_METHOD_HF) return TCG_OK;
     const size_t N = h.N;
     const int ns = h.nspin;
     const GridDesc &g = c->gd;
@@ -1264,6 +1377,20 @@ static int state_terms(tcg_ctx *c)
     RecipC rc;
     memcpy(rc.R, h.recip, sizeof rc.R);
     const unsigned pblocks = (unsigned)std::min<size_t>(148 * 8, (N + 255) / 256);
+    if (h.method == TCG_METHOD_HF) {
+        // Hartree potential of hf2h (calc_hamiltonian_hf2h.cpp:40-51)
+        TRY(c->VH.ensure(N * sizeof(double2)));
+        TRY(launch(c, k_zero, dim3(pblocks), dim3(256), 0, c->VH.as<double2>(), N));
+        TRY(launch(c, k_add, dim3(pblocks), dim3(256), 0, N, (const double2 *)c->dens.as<double2>(), c->VH.as<double2>()));
+        TRY(launch(c, k_add, dim3(pblocks), dim3(256), 0, N, (const double2 *)(c->dens.as<double2>() + N),
+                   c->VH.as<double2>()));
+        std::vector<void *> gv{c->VH.p};
+        TRY((fft3_list<double, -1>(c, gv)));
+        TRY(launch(c, k_hartree_g, dim3(pblocks), dim3(256), 0, g, rc, c->VH.as<double2>()));
+        TRY((fft3_list<double, +1>(c, gv)));
+        TCG_CUDA(cudaStreamSynchronize(c->stream));
+        return TCG_OK;
+    }
     // density in G
     DBuf &nG = c->nGw;
     TRY(nG.ensure(2 * N * sizeof(double2)));
@@ -1302,6 +1429,27 @@ static int state_terms(tcg_ctx *c)
         TRY(launch(c, k_gdot, dim3(pblocks), dim3(256), 0, g, rc, J, s1, ns, (const double2 *)W.as<double2>(),
                    (const double2 *)(W.as<double2>() + (ns > 1 ? 3 * N : 0)), V3, 0, 0));
         std::vector<void *> gv{V3};
+        TRY((fft3_list<double, +1>(c, gv)));
+    }
+    // tc2h potential (calc_hamiltonian_tc2h.cpp:53-186); its [2b_h1] dnu is the
+    // tc3a1 dnu above (same spin sum of u(G; s, js) G_d n_js(G))
+    TRY(c->V2h.ensure((size_t)ns * N * sizeof(double2)));
+    TRY(c->pgw.ensure((size_t)ns * 3 * N * sizeof(double2)));
+    for (int s = 0; s < ns; s++) {
+        const size_t g0 = h.occ_off[(size_t)s * h.nk_all];
+        const size_t g1 = s + 1 < ns ? h.occ_off[(size_t)(s + 1) * h.nk_all] : h.nocc_grids;
+        double2 *pg = c->pgw.as<double2>() + (size_t)s * 3 * N;
+        const V *chi = (h.method == TCG_METHOD_BITC ? c->Rchi.as<V>() : c->Rocc.as<V>()) + g0 * N;
+        TRY(launch(c, k_phiq_gphiq<T>, dim3(pblocks), dim3(256), 0, (int)N, (int)(g1 - g0), chi,
+                   (const V *)(c->Rgrad.as<V>() + g0 * 3 * N), (const double *)(c->occfill.as<double>() + g0), pg));
+        std::vector<void *> gp{pg, pg + N, pg + 2 * N};
+        TRY((fft3_list<double, -1>(c, gp)));
+    }
+    for (int s = 0; s < ns; s++) {
+        double2 *V2 = c->V2h.as<double2>() + (size_t)s * N;
+        TRY(launch(c, k_tc2h_g, dim3(pblocks), dim3(256), 0, g, rc, J, s, ns, (const double2 *)nG.as<double2>(),
+                   (const double2 *)c->pgw.as<double2>(), V2));
+        std::vector<void *> gv{V2};
         TRY((fft3_list<double, +1>(c, gv)));
     }
     // tc3a3b3b4b6 3b6 divergence pieces: tR_s(r), t1[s][k]
@@ -1348,7 +1496,7 @@ static int apply_impl(tcg_ctx *c, const ApplyArgs &A)
     Targets Tg = make_targets(c, A);
     const size_t nt = Tg.s.size();
     if (nt == 0) return TCG_OK;
-    const bool need_grad = (A.mask & TCG_TERM_TC2X) != 0;
+    const bool need_grad = (A.mask & (TCG_TERM_TC2X | TCG_TERM_TC2H)) != 0;
     TRY(c->Rpsi.ensure(nt * N * sizeof(V)));
     if (need_grad) TRY(c->Rgpsi.ensure(nt * 3 * N * sizeof(V)));
     {
@@ -1376,24 +1524,42 @@ static int apply_impl(tcg_ctx *c, const ApplyArgs &A)
         TRY(sphere_to_r<T>(c, items));
     }
     const unsigned pblocks = (unsigned)std::min<size_t>(148 * 8, (nt * N + 255) / 256);
-    // ---- two-body terms (H2)
-    if (A.mask & (TCG_TERM_HF2X | TCG_TERM_TC2X)) {
+    // ---- two-body terms (H2): exchange (hf2x / tc2x) and Hartree (hf2h / tc2h)
+    // accumulate in one R-space grid per band, scaled by the exchange
+    // factor tbf; the Hartree terms' own factor 1/(N_k Omega) enters as a / tbf
+    if (A.mask & TCG_TERMS_H2) {
         TRY(c->acc2.ensure(nt * N * sizeof(double2)));
         TRY(launch(c, k_zero, dim3(pblocks), dim3(256), 0, c->acc2.as<double2>(), nt * N));
-        double tbf;
+        const bool exch = (A.mask & (TCG_TERM_HF2X | TCG_TERM_TC2X)) != 0;
+        double tbf = 1.0 / (h.num_kpoints * h.omega);
         if (A.mask & TCG_TERM_HF2X) {
             tbf = -4.0 * PI_D / (h.num_kpoints * h.omega);
             TRY(run_hf2x<T>(c, Tg, c->acc2.as<double2>()));
-        } else {
+        } else if (A.mask & TCG_TERM_TC2X) {
             tbf = -1.0 / (h.num_kpoints * h.omega);
             TRY(run_tc2x<T>(c, Tg, c->acc2.as<double2>()));
         }
-        if (h.nspin == 1) tbf /= 2.0;
+        if (exch && h.nspin == 1) tbf /= 2.0;
+        if (A.mask & (TCG_TERM_HF2H | TCG_TERM_TC2H)) {
+            PhaseScope ps_h(c, "ap:2h");
+            const double a = (1.0 / (h.num_kpoints * h.omega)) / tbf;
+            const bool tc = (A.mask & TCG_TERM_TC2H) != 0;
+            for (int s = 0; s < h.nspin; s++) {
+                TRange TR = targets_of(c, Tg, s);
+                if (TR.n == 0) continue;
+                const double2 *Vr = tc ? c->V2h.as<double2>() + (size_t)s * N : c->VH.as<double2>();
+                const double2 *W = tc ? c->dnu.as<double2>() + (size_t)s * 3 * N : nullptr;
+                TRY(launch(c, k_local_h2<T>, dim3((unsigned)std::min<size_t>(64, (N + 255) / 256), TR.n), dim3(256), 0,
+                           (int)N, (const V *)(c->Rpsi.as<V>() + (size_t)TR.t0 * N),
+                           (const V *)(tc ? c->Rgpsi.as<V>() + (size_t)TR.t0 * 3 * N : nullptr), Vr, W, a,
+                           c->acc2.as<double2>() + (size_t)TR.t0 * N));
+            }
+        }
         TRY(finalize_acc(c, Tg, c->acc2.as<double2>(), A.h2, tbf));
-        TRY(div_2x(c, Tg, A, A.h2));
+        if (exch) TRY(div_2x(c, Tg, A, A.h2));
     }
     // ---- three-body terms (H3)
-    const uint32_t m3 = A.mask & ~(TCG_TERM_HF2X | TCG_TERM_TC2X);
+    const uint32_t m3 = A.mask & ~TCG_TERMS_H2;
     if (m3) {
         TRY(c->acc3.ensure(nt * N * sizeof(double2)));
         double2 *acc = c->acc3.as<double2>();

@@ -170,6 +170,17 @@ struct ChunkMeta {
     const double *tab;      // [nTB*nSB][N][ntab]            (FP64 path)
     const float4 *ftab;     // [nTB*nSB][N][nrec] coefficients (mixed path)
     int nSB, ntab, nrec;
+    // pruning of band-limited grids (prune != 0): per pair its entry in the
+    // context's pencil table; pmask[entry][x + n0 y] = 1 where the pair
+    // density's support meets pencil (x, y); pperm lists the active pencils
+    // first, pnact counts them
+    const int *pent;        // [nTB*nSB]
+    const unsigned char *pmask;
+    const unsigned short *pperm;
+    const int *pnact;
+    const unsigned long long *pbits;   // [entry][x]: bit y set where pencil (x, y) is active
+    int np, prune;
+    double pfrac;           // mean active-pencil fraction of the chunk's items (host accounting)
 };
 
 template <typename T>
@@ -211,6 +222,16 @@ struct OpBase {
     // chunk with xyi_flush; the other grids go through xyi_accum.
     static constexpr bool REGACC = false;
     static constexpr bool BOUTER = false;    // one register accumulator per output grid (xyi_flush_b)
+    // 36^3 inverse XY pass (k_xyi_t6), FP32: SACC > 0 accumulates the chunk's
+    // sources in SACC shared-memory planes per CTA (xyi_sterm picks the slot
+    // of output b, -1 for none) and adds them to the FP64 accumulators once
+    // at the end (xyi_sflush), instead of one FP64 red.add per source
+    static constexpr int SACC = 0;
+    int sacc_on = 0;                         // runtime switch of the SACC path (TCG_SACC turns it on; measured
+                                             // equal to the red.add path on the C3 workload, so off by default)
+    __device__ int xyi_slot(int) const { return -1; }
+    __device__ V xyi_sterm(int, int, int, size_t, V v) const { return v; }
+    __device__ void xyi_sflush(int, int, size_t, V) const {}
     __device__ bool regacc_grid(int) const { return false; }
     __device__ V xyi_term(int, int, int, size_t, const V *v) const { return v[0]; }
     __device__ void xyi_flush(int, size_t, V) const {}
@@ -225,6 +246,17 @@ struct OpBase {
     static constexpr bool FT = sizeof(T) == 4;   // mixed path: FP32 coefficient tables
     __device__ static float comp(const float4 &c, int d) { return d == 0 ? c.x : (d == 1 ? c.y : (d == 2 ? c.z : c.w)); }
     __device__ size_t pidx(int x, int y, int z) const { return (size_t)x + (size_t)g.n0 * (y + (size_t)g.n1 * z); }
+    // Band-limited inputs (bit f of BLI) and outputs (bit o of BLO): pair
+    // densities conj(a_q) b_k of two orbitals of the plane-wave spheres of q
+    // and k, and G-space multiples of them, vanish outside the ball
+    // |G + k - q| < R_k + R_q.  With m.prune set, the pass kernels skip
+    // their pencils outside it (XYF stores, Z loads / transforms / stores,
+    // XYI loads read as zero); values there are zero up to round-off.
+    static constexpr unsigned BLI = 0, BLO = 0;
+    __device__ int pent_of(int item) const { return m.pent[pair_id(item)]; }
+    __device__ bool pact(int item, int xy) const { return m.pmask[(size_t)pent_of(item) * m.np + xy] != 0; }
+    // active rows y of column x of the item's pair (bit y)
+    __device__ unsigned long long pcol(int item, int x) const { return m.pbits[(size_t)pent_of(item) * g.n0 + x]; }
 };
 
 // =================================================================== hf2x ==
@@ -232,6 +264,7 @@ template <typename T>
 struct OpHF2X : OpBase<T> {
     using V = typename C2<T>::t;
     static constexpr const char *NAME = "hf2x";
+    static constexpr unsigned BLI = 1, BLO = 1;           // conj(phi_q) psi_k and its multiple
     static constexpr bool REGACC = true;
     __device__ bool regacc_grid(int) const { return true; }
     __device__ V xyi_term(int, int item, int, size_t p, const V *v) const
@@ -269,6 +302,7 @@ template <typename T>
 struct OpTC2X : OpBase<T> {
     using V = typename C2<T>::t;
     static constexpr const char *NAME = "tc2x";
+    static constexpr unsigned BLI = 0xF, BLO = 0xF;       // conj(chi_q) psi_k, conj(chi_q) grad psi_k
     static constexpr bool ZSPLIT = false;     // one thread per z-line measured faster here
     static constexpr bool REGACC = true;
     __device__ bool regacc_grid(int) const { return true; }
@@ -401,6 +435,9 @@ struct OpTC3A : OpBase<T> {
     static constexpr const char *NAME = "3a3b6A";
     static constexpr int NX = EQ ? 1 : 2;     // spin branches of x2 carried
     static constexpr int NF = 4, NB = 1 + 3 * NX;
+    // input 0 = conj(chi_q) psi_k and outputs 1.. = its multiples; inputs 1-3
+    // carry dnu (their products alias over the whole grid), output 0 mixes them
+    static constexpr unsigned BLI = 1, BLO = ((1u << NB) - 1) & ~1u;
     static constexpr bool REFWD = true;
     static constexpr bool ZSPLIT = false;    // one thread per z-line measured faster here
     // accumulation through xyi_accum (FP64 red.add per source), so that the
@@ -484,6 +521,26 @@ struct OpTC3A : OpBase<T> {
     {
         const int xs = EQ ? 0 : (b - 1) / 3;
         return cmul(v, __ldg(&densT[(size_t)xs * this->g.N + p]));   // orbital * n_s2 (:332)
+    }
+    // shared-memory accumulation (k_xyi_t6, FP32): slot 0 = acc, 1 + d = qsum_d
+    static constexpr int SACC = 4;
+    __device__ int xyi_slot(int b) const
+    {
+        if (b == 0) return 0;
+        const int xs = EQ ? s : (b - 1) / 3;
+        return xs == s ? 1 + (b - 1) % 3 : -1;
+    }
+    __device__ V xyi_sterm(int, int item, int b, size_t p, V v) const
+    {
+        const int si = item % this->ns;
+        const V t = cmul(v, __ldg(&Rocc[(size_t)si * this->g.N + p]));
+        return b == 0 ? cscale(t, (decltype(t.x))(fill[si] * b3)) : t;
+    }
+    __device__ void xyi_sflush(int tj, int slot, size_t p, V sum) const
+    {
+        const size_t N = this->g.N;
+        if (slot == 0) acc_red(acc + (size_t)tj * N + p, to64(sum), 1.0);
+        else acc_red(qsum + ((size_t)tj * 3 + (slot - 1)) * N + p, to64(sum), 1.0);
     }
     __device__ V *refwd_grid(int item, int b) const { return tmp2 + ((size_t)item * 3 * NX + (b - 1)) * this->g.N; }
 };
@@ -606,6 +663,7 @@ struct OpQP : OpBase<T> {
     static constexpr const char *NAME = "qp";
     static constexpr int NX = EQ ? 1 : 2;
     static constexpr int NF = BITC ? 2 : 1, NB = (BITC ? 6 : 3) * NX, GS = BITC ? 2 : 1;
+    static constexpr unsigned BLI = (1u << NF) - 1, BLO = (1u << NB) - 1;   // pair densities of occupied orbitals
     const V *Rq2, *Rq2c;          // targets phi_q2(r), chi_q2(r)  [nt][N]
     const V *Rocc, *Rchi;         // sources phi_q1, chi_q1        [ns][N]
     double2 *acc;                 // [nt][nacc][N]: 3a2[nspin], 3a4[3], 3b5[3]
@@ -695,6 +753,9 @@ template <typename T>
 struct OpBand : OpBase<T> {
     using V = typename C2<T>::t;
     static constexpr const char *NAME = "band";
+    // input 0 = conj(chi_q2) psi_k and outputs 0-2 = its multiples; inputs 1-3
+    // carry the rotated intermediates Bt (whole grid), output 3 mixes them
+    static constexpr unsigned BLI = 1, BLO = 7;
     static constexpr bool ZSPLIT = false;     // one thread per z-line measured faster here
     static constexpr bool REGACC = true;
     __device__ bool regacc_grid(int) const { return true; }

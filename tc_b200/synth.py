@@ -20,7 +20,7 @@ Helper conventions follow TC++: k fractional, Cartesian = recip^T k
 """
 import numpy as np
 
-from .system import TCSystem
+from .system import Pseudo, TCSystem
 
 FOURPI = 4.0 * np.pi
 
@@ -369,3 +369,46 @@ def small(method="TC", nr=(12, 12, 12), nk=2, ecut=2.5, nbands=3, nocc=2, seed=0
     return build(lattice=lattice_fcc(10.26), kvec_irr=kvec, ecut=ecut, nr=nr, nbands=nbands,
                  nocc=nocc, method=method, seed=seed, left_seed=(seed + 101 if method == "BITC" else None),
                  A=A, F=F, nspin=nspin, name=f"small-{method}", **kw)
+
+
+def pseudo(sysm, seed=0, with_local=True):
+    """Synthetic pseudopotential with the shape of the reference's Si test
+    potential (one species, two projectors with l = 0 and l = 1, D_ij diagonal
+    in l; test/example*/Si_test.upf has 2 projectors): smooth seeded radial
+    factors times real spherical harmonics of k+G, atoms at (0,0,0) and
+    (1/4,1/4,1/4) of the cell, and a smooth real local potential."""
+    rng = np.random.default_rng(seed)
+    frac = np.array([[0.0, 0.0, 0.0], [0.25, 0.25, 0.25]])
+    pos = frac @ np.asarray(sysm.lattice)
+    lbeta = [[0, 1]]
+    d = rng.standard_normal(2)
+    dij = [np.diag(d)]
+    radial = rng.uniform(0.5, 1.5, size=2)
+    proj = []
+    mills = sysm.meta.get("mills")
+    for k in range(sysm.nk_irr):
+        gi, _ = sysm.gidx(0, int(sysm.kall_off[k]))
+        n = np.array(sysm.nr)
+        w = np.stack([gi % n[0], (gi // n[0]) % n[1], gi // (n[0] * n[1])], 1)
+        m = np.where(w > n // 2, w - n, w)
+        kg = (np.asarray(sysm.kvec[int(sysm.kall_off[k])])[None, :] + m) @ np.asarray(sysm.recip)
+        q = np.linalg.norm(kg, axis=1)
+        qs = np.where(q > 1e-12, q, 1.0)
+        comps = [np.exp(-radial[0] * q ** 2 / 4) / np.sqrt(FOURPI) + 0j]                   # l = 0
+        f1 = q * np.exp(-radial[1] * q ** 2 / 4) * np.sqrt(3.0 / FOURPI)
+        for dd in range(3):                                                             # l = 1, m = x, y, z
+            comps.append(-1j * f1 * kg[:, dd] / qs)
+        proj.append(np.stack(comps).ravel())
+    vloc = None
+    if with_local:
+        N = sysm.N
+        x = np.arange(N)
+        n0, n1, n2 = sysm.nr
+        i0, i1, i2 = x % n0, (x // n0) % n1, x // (n0 * n1)
+        vloc = np.zeros(N)
+        for _ in range(4):
+            h = rng.integers(-2, 3, size=3)
+            vloc += rng.standard_normal() * np.cos(2 * np.pi * (h[0] * i0 / n0 + h[1] * i1 / n1 + h[2] * i2 / n2)
+                                                   + rng.uniform(0, 2 * np.pi))
+    return Pseudo(vloc=vloc, species_of_atom=np.zeros(2, dtype=np.int32), atom_pos=pos, lbeta=lbeta, dij=dij,
+                  projector=np.concatenate(proj))

@@ -186,3 +186,38 @@ class TCSystem:
                             e = np.vdot(chi, self.band_view(h3, s, k, b))
                             e3 += f * (np.conj(e) if tr else e) / 3.0
         return e2 / self.num_kpoints, e3 / self.num_kpoints
+
+
+@dataclass
+class Pseudo:
+    """Pseudopotential data as calc_hamiltonian::pseudo reads it
+    (calc_hamiltonian_pseudo.cpp:6-180): local potential on the FFT grid,
+    atoms, per-species projector l and D_ij, and per irreducible k the
+    projector values <beta_{ip,m}|k+G> at the k's plane waves."""
+    vloc: Optional[np.ndarray]          # (N,) float64 or None
+    species_of_atom: np.ndarray         # (natoms,) int32
+    atom_pos: np.ndarray                # (natoms, 3) Cartesian bohr
+    lbeta: list                         # per species: list of l
+    dij: list                           # per species: (nproj, nproj) float64
+    projector: np.ndarray               # flat complex128 [nk][ncomp][npw_k]
+
+    def descriptor(self):
+        import ctypes as C
+        c = lambda a, dt: np.ascontiguousarray(a, dtype=dt)
+        keep = dict(vloc=None if self.vloc is None else c(self.vloc, np.float64),
+                    sp=c(self.species_of_atom, np.int32), pos=c(self.atom_pos, np.float64),
+                    nproj=c([len(l) for l in self.lbeta], np.int32),
+                    lb=c([x for l in self.lbeta for x in l], np.int32),
+                    dij=c(np.concatenate([np.asarray(d, dtype=np.float64).ravel() for d in self.dij]), np.float64),
+                    proj=c(self.projector, np.complex128))
+        d = abi.PseudoDesc()
+        d.vloc = abi.ptr(keep["vloc"], C.c_double)
+        d.nspecies = len(self.lbeta)
+        d.natoms = len(self.species_of_atom)
+        d.species_of_atom = abi.ptr(keep["sp"], C.c_int32)
+        d.atom_pos = abi.ptr(keep["pos"], C.c_double)
+        d.nproj = abi.ptr(keep["nproj"], C.c_int32)
+        d.lbeta = abi.ptr(keep["lb"], C.c_int32)
+        d.dij = abi.ptr(keep["dij"], C.c_double)
+        d.projector = abi.ptr(keep["proj"].view(np.float64), C.c_double)
+        return d, keep

@@ -12,8 +12,8 @@ test, so the fixture holds
   - E2, E3: the oracle's two- and three-body energies (total_energy.cpp:101-168,
     e_n = <chi_i|H_n phi_i>) from H applied to all occupied orbitals.
 The GPU tests and bench.py compare the CUDA path (FP64 and mixed precision)
-against these numbers.  Run from the repository root (about half an hour on
-eight cores):
+against these numbers.  Run from the repository root (on
+eight cores, about an hour):
 
     python tests/golden/make_c3_subset.py
 """

@@ -290,3 +290,52 @@ def test_unequal_channels_spin_polarised():
         g2, g3 = ctx.apply(abi.TERMS_TC)
     assert rel(g2, r2) < FP64_TOL
     assert rel(g3, r3) < FP64_TOL
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+@pytest.mark.parametrize("method,term", [("HF", "hf2h"), ("TC", "tc2h"), ("BITC", "tc2h")])
+def test_hartree_terms(method, term, prec, tol):
+    """hf2h / tc2h (local potentials of the density) on the device vs the oracle,
+    alone and together with the exchange term of the same H2 accumulator"""
+    s = system(method)
+    bit = abi.TERM_NAMES_EXTRA[term]
+    for mask in (bit, bit | (abi.TERM_HF2X if method == "HF" else abi.TERM_TC2X)):
+        r2, _ = O.apply(s, mask)
+        with Context(s, prec) as ctx:
+            ctx.set_state()
+            g2, _ = ctx.apply(mask)
+        assert rel(g2, r2) < tol
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+@pytest.mark.parametrize("tr", [False, True])
+def test_one_body_terms(prec, tol, tr):
+    """kinetic + pseudopotential (non-local projectors, local potential) vs the oracle"""
+    s = system("TC", tr=tr, nr=(16, 16, 16), ecut=1.5, nbands=2, nocc=1) if tr else system("TC")
+    pp = synth.pseudo(s, seed=44)
+    for mask in (abi.TERM_KINETIC, abi.TERM_PSEUDO, abi.TERMS_H1):
+        ref = O.apply_h1(s, mask, pp)
+        with Context(s, prec) as ctx:
+            ctx.set_pseudo(pp)
+            got = ctx.apply_h1(mask)
+        assert rel(got, ref) < tol
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+@pytest.mark.parametrize("method", ["HF", "TC", "BITC"])
+@pytest.mark.parametrize("prune", [True, False])
+def test_36_pruned_transforms(monkeypatch, method, prune, prec, tol):
+    """36^3 default kernels with the band-limited grids pruned to the pencils
+    their support meets (default) and without (TCG_NO_PRUNE), vs the oracle;
+    a cutoff large enough that the support balls cover a good part of the grid"""
+    if not prune:
+        monkeypatch.setenv("TCG_NO_PRUNE", "1")
+    s = system(method, nr=(36, 36, 36), nk=2, ecut=6.0, nbands=2, nocc=1)
+    mask = abi.TERMS_HF if method == "HF" else abi.TERMS_TC
+    r2, r3 = oracle_terms(s, mask)
+    with Context(s, prec) as ctx:
+        ctx.set_state()
+        g2, g3 = ctx.apply(mask)
+    assert rel(g2, r2) < tol
+    if method != "HF":
+        assert rel(g3, r3) < tol

@@ -7,9 +7,10 @@ n = sum f chi* phi (bloch_states_scfloop_filling_density.cpp:256-360).  E is a
 polynomial in conj(chi) of degree 2 (two-body) and 3 (three-body); if H2 and
 H3 are the mean-field derivatives of E2 and E3, Euler's theorem gives
     dE / d conj(chi_i)(G) = f_i / N_k (H2 + H3) phi_i (G).
-This holds for tc2x alone, for tc3a1 + tc3b1 together and for tc3a2a4b2b5 +
-tc3a3b3b4b6 together (the reference splits each three-body derivative over
-two routines), so a wrong factor or sign in any term breaks it.  Checked by
+This holds for tc2x, tc2h, hf2x and hf2h alone, for tc3a1 + tc3b1 together
+and for tc3a2a4b2b5 + tc3a3b3b4b6 together (the reference splits each
+three-body derivative over two routines), so a wrong factor or sign in any
+term breaks it.  Checked by
 central finite differences (h = 1e-5) of the oracle's energy, with the
 density recomputed from the perturbed orbitals: E depends on chi only through
 conj(chi), so d/dRe chi = dE/d conj(chi) and d/dIm chi = -i dE/d conj(chi).
@@ -23,8 +24,9 @@ from tc_b200 import abi, synth
 from oracle import oracle as O
 
 H = 1e-5
-GROUPS = {"tc2x": ["tc2x"], "tc3a1+tc3b1": ["tc3a1", "tc3b1"],
-          "tc3a2a4b2b5+tc3a3b3b4b6": ["tc3a2a4b2b5", "tc3a3b3b4b6"], "hf2x": ["hf2x"]}
+GROUPS = {"tc2x": ["tc2x"], "tc2h": ["tc2h"], "tc3a1+tc3b1": ["tc3a1", "tc3b1"],
+          "tc3a2a4b2b5+tc3a3b3b4b6": ["tc3a2a4b2b5", "tc3a3b3b4b6"], "hf2x": ["hf2x"], "hf2h": ["hf2h"]}
+NAMES = dict(abi.TERM_NAMES, **abi.TERM_NAMES_EXTRA)
 
 
 def energy(s, mask):
@@ -54,11 +56,11 @@ def perturbed(s, field, off, d):
 
 @pytest.mark.parametrize("group", list(GROUPS))
 def test_operator_is_energy_gradient(group):
-    method = "HF" if group == "hf2x" else "BITC"
+    method = "HF" if group.startswith("hf") else "BITC"
     s = synth.small(method, nk=2, nr=(12, 12, 12), ecut=2.0, nbands=2, nocc=2, seed=7)
     mask = 0
     for t in GROUPS[group]:
-        mask |= abi.TERM_NAMES[t]
+        mask |= NAMES[t]
     field = "phik_left" if method == "BITC" else "phik"
     _, h2, h3 = energy(s, mask)
     rng = np.random.default_rng(3)
