@@ -140,7 +140,7 @@ def run_ours(args):
     import torch.distributed as dist
     from tc_b200 import abi, synth
     from tc_b200.context import Context
-    from tc_b200.sharding import sharded_qp_stage
+    from tc_b200.sharding import reduce_h, sharded_qp_stage
 
     world, rank, local = dist_info()
     torch.cuda.set_device(local)
@@ -185,6 +185,9 @@ def run_ours(args):
             torch.cuda.synchronize()
             state()
             ctx.apply_device(mask, psi_dev.data_ptr(), h2.data_ptr(), h3.data_ptr(), owned=owned)
+            if world > 1:
+                with torch.cuda.stream(stream):
+                    reduce_h([h2, h3])
 
         for _ in range(warmup):
             step()
@@ -206,6 +209,9 @@ def run_ours(args):
             e0.record(stream)
             state()
             ctx.apply_device(mask, psi_dev.data_ptr(), h2.data_ptr(), h3.data_ptr(), owned=owned)
+            if world > 1:
+                with torch.cuda.stream(stream):
+                    reduce_h([h2, h3])      # calc_hamiltonian::all's reduction of H phi over ranks
             e1.record(stream)
             torch.cuda.nvtx.range_pop()
             torch.cuda.synchronize()

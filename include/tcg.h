@@ -239,6 +239,48 @@ int tcg_energy(tcg_ctx *ctx, const int32_t *nb_apply, const void *h2_dev, const 
 int tcg_energy_grad(tcg_ctx *ctx, uint32_t term_mask, double *e_out, void *dE_dchi_dev, double *dE_du,
                     double *dE_dv2);
 
+/* Rayleigh-Ritz step of the block Davidson for one (spin, k) block, on the
+ * device in FP64 (Diagonalization::block_davidson,
+ * diagonalization_davidson.cpp:462-600):
+ *   H_n,sub = Vref^H (H_n V)  for the given n = 1, 2, 3 (ZGEMM),
+ *   H_sub = sum_n H_n,sub,  H_sub X = X D  (general complex eigensolve;
+ *   ComplexEigenSolver in the reference), eigenpairs sorted by the real part
+ *   (sort_eigen, diagonalization_utils.cpp:82-119), X_left = (X^-1)^H,
+ *   V_out = V X[:, :nout],  Vl_out = Vref X_left[:, :nout] (if non-NULL),
+ *   e_out[3][nout] = diag(L^H H_n,sub X), L = X_left if biortho else X.
+ * V, Vref (NULL: V), H1V, H2V, H3V (NULL: absent): DEVICE [ndim][npw]
+ * complex, one basis vector after the other; eig_out [ndim] and e_out
+ * [3][nout] complex on the host (e_out may be NULL); V_out, Vl_out DEVICE
+ * [nout][npw].  `stream` is a cudaStream_t (NULL: default); the call returns
+ * after the work finished.  Scratch is allocated and freed per call. */
+int tcg_subspace_ritz(int32_t ndim, int32_t npw, int32_t nout, int32_t biortho, const void *V, const void *Vref,
+                      const void *H1V, const void *H2V, const void *H3V, double *eig_out, double *e_out,
+                      void *V_out, void *Vl_out, void *stream);
+
+/* Gram-Schmidt orthonormalisation of nvec DEVICE vectors V [nvec][npw] in
+ * place, in order (Diagonalization::Gram_Schmidt, diagonalization_utils.cpp:
+ * 7-28); with Vl non-NULL the bi-orthonormalisation of (V, Vl), <Vl_i|V_j> =
+ * delta_ij (Gram_Schmidt_biortho, :30-77).  TCG_ERR_NUMERIC when a vector
+ * becomes linearly dependent (norm < 1e-8, 1e-10 bi-orthogonal), as the
+ * reference stops there. */
+int tcg_gram_schmidt(int32_t nvec, int32_t npw, void *V, void *Vl, void *stream);
+
+/* New trial vectors of one block-Davidson block for one (spin, k), on the
+ * device in FP64 (diagonalization_davidson.cpp:283-318 with
+ * Diagonalization::make_a_new_trial_vector, diagonalization_utils.cpp:
+ * 165-211): for each b < nblock the preconditioned residual
+ * -K(|k+G|^2 / t_b) (H1 + H2 + H3 - e_b) phi_b, t_b the kinetic expectation of
+ * phi_b, normalised; then orthonormalised against the rows of V in order
+ * (the new rows of this call included) and appended as row *nbasis_out of V,
+ * unless its norm falls below 1e-8, in which case it is dropped.
+ * V: DEVICE [nbasis + nblock][npw] (capacity), rows < nbasis the current
+ * orthonormal basis; phi, H1phi, H2phi, H3phi (NULL: absent): DEVICE
+ * [nblock][npw]; kG2: DEVICE [npw] |k+G|^2; eig_ref: host complex [nblock],
+ * the eigenvalues of the previous iteration.  Returns after the work. */
+int tcg_davidson_expand(int32_t nbasis, int32_t nblock, int32_t npw, void *V, const void *phi, const void *H1phi,
+                        const void *H2phi, const void *H3phi, const double *kG2, const double *eig_ref,
+                        int32_t *nbasis_out, void *stream);
+
 /* Divergence-correction scalars for the SCF mesh (Potentials::set_sum_of_Vaux
  * with set_sum_of_Vaux_each, potentials_coulomb.cpp:60-161), computed on the
  * device.  Writes alpha_Vaux and sum_Vaux[nk_irr]; needs only the geometry

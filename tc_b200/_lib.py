@@ -50,6 +50,11 @@ def lib():
         L.tcg_set_pseudo.argtypes = [vp, C.POINTER(abi.PseudoDesc)]
         L.tcg_apply_h1.argtypes = [vp, C.c_uint32, C.POINTER(C.c_int32), vp, vp, vp]
         L.tcg_energy_grad.argtypes = [vp, C.c_uint32, C.POINTER(C.c_double), vp, vp, vp]
+        L.tcg_subspace_ritz.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, vp,
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double), vp, vp, vp]
+        L.tcg_gram_schmidt.argtypes = [C.c_int32, C.c_int32, vp, vp, vp]
+        L.tcg_davidson_expand.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp,
+                                          C.POINTER(C.c_double), C.POINTER(C.c_int32), vp]
         L.tcg_energy.argtypes = [vp, C.POINTER(C.c_int32), vp, vp, C.POINTER(C.c_double)]
         _lib = L
     return _lib
@@ -63,4 +68,5 @@ def check(rc):
 EXPORTS = ["tcg_ctx_create", "tcg_ctx_destroy", "tcg_set_state", "tcg_apply", "tcg_apply_device",
            "tcg_sum_of_vaux", "tcg_density", "tcg_stream", "tcg_launch_count", "tcg_last_error",
            "tcg_version", "tcg_set_tuning", "tcg_profile", "tcg_profile_read", "tcg_refresh_state",
-           "tcg_sum_of_vaux_noalloc", "tcg_energy", "tcg_qp_partial", "tcg_qp_finish", "tcg_set_pseudo", "tcg_apply_h1", "tcg_energy_grad"]
+           "tcg_sum_of_vaux_noalloc", "tcg_energy", "tcg_qp_partial", "tcg_qp_finish", "tcg_set_pseudo", "tcg_apply_h1", "tcg_energy_grad",
+           "tcg_subspace_ritz", "tcg_gram_schmidt", "tcg_davidson_expand"]

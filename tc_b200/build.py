@@ -1,8 +1,9 @@
 """Build step of the CUDA library libtcg_b200.so (in-tree, sm_100a).
 
-api.cu (C-ABI, orchestration, generic kernels) and one instance of
-fast_inst.cu per compiled cubic grid size are compiled in parallel into
-tc_b200/_build/ and linked into tc_b200/libtcg_b200.so.
+api.cu (C-ABI, orchestration, generic kernels), subspace.cu (the dense
+Davidson subspace step on cuBLAS / cuSOLVER) and one instance of fast_inst.cu
+per compiled cubic grid size are compiled in parallel into tc_b200/_build/
+and linked into tc_b200/libtcg_b200.so.
 """
 import concurrent.futures as cf
 import os
@@ -31,7 +32,8 @@ def stale():
 
 
 def _units():
-    units = [(os.path.join(SRC, "api.cu"), os.path.join(OBJ, "api.o"), [])]
+    units = [(os.path.join(SRC, "api.cu"), os.path.join(OBJ, "api.o"), []),
+             (os.path.join(SRC, "subspace.cu"), os.path.join(OBJ, "subspace.o"), [])]
     for n in FAST_SIZES:
         units.append((os.path.join(SRC, "fast_inst.cu"), os.path.join(OBJ, f"fast_{n}.o"), [f"-DTCG_FAST_N={n}"]))
     return units
@@ -57,7 +59,7 @@ def build(force=False, verbose=False, jobs=None):
     jobs = jobs or min(len(units), os.cpu_count() or 4)
     with cf.ThreadPoolExecutor(jobs) as ex:
         objs = list(ex.map(compile_one, units))
-    cmd = [nvcc, *ARCH, "-shared", "-o", SO + ".tmp", *objs]
+    cmd = [nvcc, *ARCH, "-shared", "-o", SO + ".tmp", *objs, "-lcublas", "-lcusolver"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

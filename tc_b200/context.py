@@ -214,3 +214,52 @@ def sum_of_vaux_noalloc(system, kirr_dev_ptr, kall_dev_ptr, out_dev_ptr, stream=
 
 def version():
     return lib().tcg_version().decode()
+
+
+def subspace_ritz(V, HV, nout, Vref=None, biortho=False, stream=None, left=False):
+    """Rayleigh-Ritz step of the block Davidson on the device (tcg_subspace_ritz).
+    V, Vref: torch complex128 CUDA tensors [ndim, npw]; HV: list of up to three
+    tensors [ndim, npw] (H1 V, H2 V, H3 V; None for absent).  Returns
+    (eigenvalues [ndim], energies [3, nout], V_out [nout, npw], Vl_out or None);
+    the left vectors Vref X_left are computed when Vref is given or left is set."""
+    import torch
+    ndim, npw = V.shape
+    hv = list(HV) + [None] * (3 - len(HV))
+    ptr = lambda x: None if x is None else C.c_void_p(x.data_ptr())
+    eig = np.zeros(ndim, dtype=np.complex128)
+    en = np.zeros((3, max(nout, 1)), dtype=np.complex128)
+    Vo = torch.zeros((max(nout, 1), npw), dtype=torch.complex128, device=V.device)
+    Vl = torch.zeros_like(Vo) if (Vref is not None or left) else None
+    check(lib().tcg_subspace_ritz(int(ndim), int(npw), int(nout), 1 if biortho else 0, ptr(V), ptr(Vref),
+                                  ptr(hv[0]), ptr(hv[1]), ptr(hv[2]),
+                                  eig.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)),
+                                  en.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)), ptr(Vo), ptr(Vl),
+                                  None if stream is None else C.c_void_p(stream)))
+    return eig, en[:, :nout], Vo[:nout], (None if Vl is None else Vl[:nout])
+
+
+def gram_schmidt(V, Vl=None, stream=None):
+    """In-place Gram-Schmidt (or bi-orthonormalisation with Vl) of the rows of
+    the torch complex128 CUDA tensor V [nvec, npw] (tcg_gram_schmidt)."""
+    nvec, npw = V.shape
+    check(lib().tcg_gram_schmidt(int(nvec), int(npw), C.c_void_p(V.data_ptr()),
+                                 None if Vl is None else C.c_void_p(Vl.data_ptr()),
+                                 None if stream is None else C.c_void_p(stream)))
+
+
+def davidson_expand(V, nbasis, phi, H, kG2, eig_ref, stream=None):
+    """New trial vectors of one Davidson block (tcg_davidson_expand): V torch
+    complex128 CUDA [capacity, npw] with nbasis valid rows; phi [nblock, npw];
+    H: list of up to three [nblock, npw] (H1 phi, H2 phi, H3 phi, None for
+    absent); kG2 float64 CUDA [npw]; eig_ref complex [nblock] (host).  Returns
+    the new number of valid rows of V."""
+    nblock, npw = phi.shape
+    h = list(H) + [None] * (3 - len(H))
+    ptr = lambda x: None if x is None else C.c_void_p(x.data_ptr())
+    e = np.ascontiguousarray(np.asarray(eig_ref, dtype=np.complex128)[:nblock])
+    out = C.c_int32()
+    check(lib().tcg_davidson_expand(int(nbasis), int(nblock), int(npw), ptr(V), ptr(phi), ptr(h[0]), ptr(h[1]),
+                                    ptr(h[2]), ptr(kG2), e.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)),
+                                    C.byref(out), None if stream is None else C.c_void_p(stream)))
+    return int(out.value)
+

@@ -647,8 +647,10 @@ static int finalize_acc(tcg_ctx *c, const Targets &T, double2 *acc, double2 *hou
         gi[t].fac = make_double2(fac / (double)N, 0.0);
     }
     TRY(c->items.ensure(nt * (sizeof(void *) + sizeof(GatherItem))));
-    void **d_grids = c->items.as<void *>();
-    GatherItem *d_gi = reinterpret_cast<GatherItem *>(d_grids + nt);
+    // the items first: GatherItem holds a double2 (16-byte aligned), the
+    // pointer array after them (8-byte aligned whatever nt is)
+    GatherItem *d_gi = c->items.as<GatherItem>();
+    void **d_grids = reinterpret_cast<void **>(d_gi + nt);
     TCG_CUDA(cudaMemcpyAsync(d_grids, grids.data(), nt * sizeof(void *), cudaMemcpyHostToDevice, c->stream));
     TCG_CUDA(cudaMemcpyAsync(d_gi, gi.data(), nt * sizeof(GatherItem), cudaMemcpyHostToDevice, c->stream));
     const int ntiles = (g.n0 * g.n1 + ZTC - 1) / ZTC;

@@ -46,6 +46,8 @@ class QEData:
         self.nr = (int(fg["nr1"]), int(fg["nr2"]), int(fg["nr3"]))
         self.gamma_only = bs.find("gamma_only").text.strip() == "true"
         self.atoms = [(a.attrib["name"], _floats(a.text)) for a in ast.find("atomic_positions")]
+        self.pseudo_files = {sp.attrib["name"]: sp.find("pseudo_file").text.strip()
+                             for sp in out.find("atomic_species").findall("species")}
         rots, trans = [], []
         for sym in out.find("symmetries").findall("symmetry"):
             if sym.find("equivalent_atoms") is None:
@@ -83,6 +85,8 @@ class QEData:
 
     def save_npz(self, path):
         d = {f: np.asarray(getattr(self, f)) for f in self._FIELDS}
+        d["atom_names"] = np.array([n for n, _ in self.atoms])
+        d["atom_pos"] = np.array([p for _, p in self.atoms])
         for ik in range(len(self.kweight)):
             m, c = self.read_wfc(ik)
             d[f"mill_{ik}"], d[f"evc_{ik}"], d[f"eig_{ik}"], d[f"occ_{ik}"] = m, c, self.eig[ik], self.occ[ik]
@@ -101,6 +105,8 @@ class QEData:
         q.kweight = [float(w) for w in q.kweight]
         q.eig = [z[f"eig_{ik}"] for ik in range(nk)]
         q.occ = [z[f"occ_{ik}"] for ik in range(nk)]
+        q.atoms = [(str(n), p) for n, p in zip(z["atom_names"], z["atom_pos"])] if "atom_names" in z else []
+        q.pseudo_files = {}
         q._wfc = [(z[f"mill_{ik}"], z[f"evc_{ik}"]) for ik in range(nk)]
         return q
 

@@ -1,6 +1,6 @@
 """Multi-rank host logic: one process per GPU.
 
-Two pieces of the reference's MPI parallelisation are mirrored:
+Three pieces of the reference's MPI parallelisation are mirrored:
   - the (spin, k, band) targets of an apply are split over ranks by k-point,
     round robin, through the ownership mask of tcg_apply
     (Parallelization::set_orbital_parallelization, parallelization.cpp:127-172);
@@ -9,7 +9,11 @@ Two pieces of the reference's MPI parallelisation are mirrored:
     before the rotation / local-potential half runs on every rank
     (calc_hamiltonian_tc3a2a4b2b5.cpp:214-235 split, :490-493 and :649-659
     MPI_Allreduce).  The sum is one torch.distributed all_reduce (NCCL on the
-    GPU) of the library's device buffer.
+    GPU) of the library's device buffer;
+  - the reduction of H phi over ranks that closes calc_hamiltonian::all
+    (MPI_Reduce to rank 0, calc_hamiltonian_all.cpp:164-197): each rank's
+    packed H1 / H2 / H3 holds its own bands (zero elsewhere), and
+    reduce_h sums them with one collective per array, on the device.
 """
 import numpy as np
 
@@ -55,3 +59,19 @@ def sharded_qp_stage(ctx, group=None, view=None):
     if buf.is_cuda:
         torch.cuda.synchronize(buf.device)
     ctx.qp_finish()
+
+
+def reduce_h(arrays, group=None, dst=None):
+    """Sum the ranks' packed H phi arrays (torch tensors, complex128 or their
+    float64 views; on the GPU for NCCL) in place: all ranks receive the sum
+    (dst None) or only rank dst (the reference's MPI_Reduce to rank 0)."""
+    import torch
+    import torch.distributed as dist
+    for a in arrays:
+        if a is None:
+            continue
+        buf = torch.view_as_real(a) if a.is_complex() else a
+        if dst is None:
+            dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
+        else:
+            dist.reduce(buf, dst=dst, op=dist.ReduceOp.SUM, group=group)

@@ -1,0 +1,73 @@
+"""Oracle pinned to the reference's own outputs: the first SCF iteration of
+TC++'s test runs test/example1 (HF), test/example2 (TC) and test/example3
+(BITC) replayed on the CPU.
+
+Input: the Quantum ESPRESSO orbitals of fcc Si those runs start from (16^3
+grid, 3 irreducible k-points expanded by 48 space-group operations, half with
+the fractional translation (1/4, 1/4, 1/4), and time reversal), Si_test.upf and
+the RPA F of each run's parameters.casl (tests/golden/make_si_examples.py).
+H phi of every term comes from the oracle (hf2x, hf2h, tc2x, tc2h, tc3a1,
+tc3b1, tc3a2a4b2b5, tc3a3b3b4b6, kinetic, local and non-local
+pseudopotential), the block-Davidson step, the SCF update between two
+iterations (new orbitals, fixed occupations, mixed density) and the energy
+functional from tests/_replay.py.  The 1-, 2- and 3-body energies of both
+SCF iterations the runs made must equal the ones TC++ printed (output.out,
+"Total energy (n-body terms)"), real and imaginary parts, to 1e-8 Ha; the
+reference's own tests accept 1e-5 (test/test.py).  The orbital energies must
+match to the printed digits apart from TC++'s Hartree-to-eV factor (the same
+for every band).
+"""
+import numpy as np
+import pytest
+
+import _replay as R
+
+TOL = 1e-8
+
+
+@pytest.fixture(scope="module", params=["example1", "example2", "example3"])
+def replay(request):
+    s, pp, eig, rec = R.si_system(request.param)
+    e, en = R.davidson(s, R.oracle_apply(s, pp), eig)
+    s2 = R.scf_update(s, e, nelec=8.0)
+    e2, en2 = R.davidson(s2, R.oracle_apply(s2, pp), e)
+    return [(s, e, en), (s2, e2, en2)], rec
+
+
+@pytest.mark.parametrize("it", [0, 1])
+def test_energies_match_reference_output(replay, it):
+    runs, rec = replay
+    s, e, en = runs[it]
+    E = R.total_energy(s, e, en, nelec=8.0)
+    gold = rec["iterations"][it]
+    for n, key in enumerate(("1-body", "2-body", "3-body")):
+        if key not in gold:
+            assert s.method == "HF" and E[n] == 0
+            continue
+        ref = complex(*gold[key])
+        assert abs(E[n].real - ref.real) <= TOL, (key, E[n], ref)
+        assert abs(E[n].imag - ref.imag) <= TOL, (key, E[n], ref)
+
+
+def test_orbital_energies_match_reference_output(replay):
+    runs, rec = replay
+    s, e, en = runs[0]
+    ev = np.array(rec["iterations"][0]["orbital_energies_eV"])
+    ratio = ev / e.real
+    # one Hartree-to-eV factor for every band, equal to the CODATA value to 1e-7
+    assert np.ptp(ratio) <= 1e-8 * np.abs(ratio).max() + 2e-9 / np.abs(e.real).min()
+    assert abs(np.median(ratio) / 27.211386245988 - 1) < 1e-7
+
+
+def test_planted_error_is_caught():
+    """A 1e-6 relative error in one term's H phi moves the energy beyond TOL."""
+    s, pp, eig, rec = R.si_system("example3")
+    base = R.oracle_apply(s, pp)
+
+    def bad(psi, nba):
+        h1, h2, h3 = base(psi, nba)
+        return h1, h2, h3 * (1 + 1e-6)
+    e, en = R.davidson(s, bad, eig)
+    E = R.total_energy(s, e, en, nelec=8.0)
+    ref = complex(*rec["iterations"][0]["3-body"])
+    assert abs(E[2] - ref) > TOL

@@ -2,7 +2,7 @@
 test/example3: 3 irreducible k-points, 48 space-group operations of which 24
 carry the fractional translation (1/4, 1/4, 1/4), time reversal), read by
 tc_b200.qe as TC++ reads it (tests/golden/qe_si.npz is the compact copy made by
-tests/golden/make_qe_fixture.py).
+tests/golden/make_si_examples.py).
 
 - The k-point star TC++ builds from it (Kpoints::set_kvectors_by_symmetry) is
   the one the reference printed for this run (test/example3/output.out:383-449).

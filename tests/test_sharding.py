@@ -37,8 +37,9 @@ def _worker(rank, world, port, q):
         s = synth.small("TC", nk=2)
         own = sharding.owned_mask(s, world, rank)
         h2, h3 = O.apply(s, abi.TERMS_TC, owned=own)
-        t = torch.from_numpy(np.concatenate([h2.view(np.float64), h3.view(np.float64)]))
-        dist.all_reduce(t)                               # union of disjoint shards
+        t2, t3 = torch.from_numpy(h2.copy()), torch.from_numpy(h3.copy())
+        sharding.reduce_h([t2, t3])                      # union of disjoint shards (all()'s reduction)
+        t = torch.from_numpy(np.concatenate([t2.numpy().view(np.float64), t3.numpy().view(np.float64)]))
         m = torch.tensor([float(own.sum()), float(rank + 1)])
         dist.all_reduce(m[1:], op=dist.ReduceOp.MAX)     # max-over-ranks timing
         masks = [torch.zeros(own.size, dtype=torch.uint8) for _ in range(world)]
