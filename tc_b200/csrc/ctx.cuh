@@ -133,6 +133,8 @@ struct tcg_ctx {
     std::vector<int> prune_nact;            // host copy of the table's active-pencil counts
     bool no_prune = false;                  // TCG_NO_PRUNE: full transforms everywhere
     bool use_sacc = false;                  // TCG_SACC: shared-memory accumulation in the 3a3b6A inverse XY pass
+    bool qp_sacc = true;                    // TCG_NO_QP_SACC clears: shared-memory accumulation in the
+                                            // occupied-pair inverse XY pass (36^3, FP32)
     tcg::DBuf Qt, Bt;                       // tc3a2a4b2b5 rotated intermediates [nocc_grids][3][N]
     tcg::DBuf accP, qtg;                    // occupied-pair accumulators / gathered q2 grids
     tcg::DBuf div3b6;                       // [nspin][N] fp64 temp_div_3b6 in R space

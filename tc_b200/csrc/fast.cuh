@@ -710,6 +710,20 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyf_t6(Op op, int nplanes)
     }
 }
 
+// shared-memory accumulation of one output group (GS outputs in vals): the
+// op's own xyi_sgroup, or its single slot xyi_slot(b0) (called on the derived
+// op type, so that its overrides apply)
+template <class Op, typename V, class F>
+__device__ __forceinline__ void sacc_group(const Op &op, int tj, int item, int b0, size_t p, const V *vals, F &&add)
+{
+    if constexpr (Op::SACC_GROUP) {
+        op.xyi_sgroup(tj, item, b0, p, vals, add);
+    } else {
+        const int slot = op.xyi_slot(b0);
+        if (slot >= 0) add(slot, op.xyi_sterm(tj, item, b0, p, vals[Op::GS - 1]));
+    }
+}
+
 // XYI: one (target, z) plane per CTA, looping over the chunk's (source,
 // output) steps; the next step's plane is copied asynchronously into the
 // second set.  GS > 1: the first GS - 1 outputs of a group wait in registers.
@@ -731,26 +745,25 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
     constexpr bool RACC = Op::REGACC && sizeof(V) == 8;
     constexpr int SA = sizeof(V) == 8 ? Op::SACC : 0;    // shared-memory accumulator planes (FP32)
     const bool sa_on = SA > 0 && op.sacc_on;
+    const int nsa = sa_on ? op.sacc_n : 0;                // planes in use
     static_assert(!(RACC && Op::REFWD), "re-forwarded outputs accumulate through xyi_accum");
     static_assert(!(Op::REFWD && Op::GS > 1), "re-forward needs GS == 1");
-    static_assert(!(SA > 0 && (RACC || Op::GS > 1)), "shared-memory accumulation replaces the other forms");
+    static_assert(!(SA > 0 && RACC), "shared-memory accumulation replaces the register form");
+    static_assert(!(SA > 0 && Op::GS > 1 && !Op::SACC_GROUP), "grouped outputs need the op's xyi_sgroup");
     V racc[R], keep[Op::GS][R];
 #pragma unroll
     for (int i = 0; i < R; i++) racc[i] = czero<V>();
     V *SAcc = W + 2 * PS;                 // [SA][N][N]: this thread owns y = t + 6 k2, x = l
     // pruned chunks: the pencil-table entry of every source, looked up once
     // (the copies of each step then need one load of their column mask)
-    int *sent = reinterpret_cast<int *>(SAcc + (sa_on ? SA * N * N : 0));
+    int *sent = reinterpret_cast<int *>(SAcc + (size_t)nsa * N * N);
     if (op.m.prune) {
         for (int si = threadIdx.x; si < ns; si += blockDim.x) sent[si] = op.pent_of(op.item_of(tj, si));
         __syncthreads();
     }
-    if (sa_on) {
+    for (int a = 0; a < nsa; a++)
 #pragma unroll
-        for (int a = 0; a < SA; a++)
-#pragma unroll
-            for (int k2 = 0; k2 < R; k2++) SAcc[(a * N + t + R * k2) * N + l] = czero<V>();
-    }
+        for (int k2 = 0; k2 < R; k2++) SAcc[(a * N + t + R * k2) * N + l] = czero<V>();
     const int total = ns * Op::NB;        // it = si * NB + b
     auto issue = [&](int it) {
         const int item = op.item_of(tj, it / Op::NB), b = it % Op::NB;
@@ -792,13 +805,17 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
         }
         const int item = op.item_of(tj, si);
         if (sa_on) {
-            const int slot = op.xyi_slot(b0);      // uniform over the CTA
-            if (slot >= 0) {
+            // this thread owns the accumulator points (x = l, y = t + 6 k2) of every slot
 #pragma unroll
-                for (int k2 = 0; k2 < R; k2++) {
+            for (int k2 = 0; k2 < R; k2++) {
+                V vals[Op::GS];
+#pragma unroll
+                for (int g = 0; g < Op::GS - 1; g++) vals[g] = keep[g][k2];
+                vals[Op::GS - 1] = v[k2];
+                sacc_group(op, tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals, [&](int slot, V x) {
                     V *a = &SAcc[(slot * N + t + R * k2) * N + l];
-                    *a = cadd(*a, op.xyi_sterm(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, v[k2]));
-                }
+                    *a = cadd(*a, x);
+                });
             }
         } else if (RACC && op.regacc_grid(b0)) {
 #pragma unroll
@@ -836,17 +853,16 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
 #pragma unroll
         for (int k2 = 0; k2 < R; k2++) op.xyi_flush(tj, pz + (size_t)(t + R * k2) * N + l, racc[k2]);
     }
-    if (sa_on) {
+    for (int a = 0; a < nsa; a++)
 #pragma unroll
-        for (int a = 0; a < SA; a++)
-#pragma unroll
-            for (int k2 = 0; k2 < R; k2++)
-                op.xyi_sflush(tj, a, pz + (size_t)(t + R * k2) * N + l, SAcc[(a * N + t + R * k2) * N + l]);
-    }
+        for (int k2 = 0; k2 < R; k2++)
+            op.xyi_sflush(tj, a, pz + (size_t)(t + R * k2) * N + l, SAcc[(a * N + t + R * k2) * N + l]);
 }
-template <typename V, class Op> __host__ inline size_t smem_xyi(int sets, bool sacc_on)
+// shared memory of k_xyi_t6: twiddles, `sets` plane sets, `slots` FP32
+// accumulator planes (0 unless the op's SACC path is on)
+template <typename V, class Op> __host__ inline size_t smem_xyi(int sets, int slots)
 {
-    return sizeof(V) * (128 + (size_t)sets * N * PAD + (sizeof(V) == 8 && sacc_on ? (size_t)Op::SACC * N * N : 0));
+    return sizeof(V) * (128 + (size_t)sets * N * PAD + (sizeof(V) == 8 ? (size_t)slots * N * N : 0));
 }
 
 // Z pass: one item and 32 consecutive pencils (x, y) per CTA, six threads

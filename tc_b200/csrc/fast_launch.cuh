@@ -70,7 +70,7 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
             const int nref = Op::REFWD ? Op::NB - 1 : 0;
             return launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (nb_eff + nref) * gb,
                                  fast::t6::k_xyi_t6<T, Op>, dim3(np_i), dim3(fast::t6::THREADS),
-                                 fast::t6::smem_xyi<V, Op>(2, op.sacc_on != 0) +
+                                 fast::t6::smem_xyi<V, Op>(2, op.sacc_on ? op.sacc_n : 0) +
                                      (op.m.prune ? (size_t)op.ns * sizeof(int) : 0),
                                  op, np_i);
         }

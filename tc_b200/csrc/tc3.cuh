@@ -881,6 +881,7 @@ static int tc3_stage_ab(tcg_ctx *c, const Targets &Tg, const TRange &TR, const S
         a.s = s;
         a.b3 = b3;
         a.sacc_on = c->use_sacc ? 1 : 0;
+        a.sacc_n = OA::SACC;
         TRY((run_chunk<T, OA>(c, a, (int)items, p.nt)));
         OB b;
         op_common<T>(c, b, p, nsl, 2);
@@ -1005,6 +1006,10 @@ static int qp_pairs(tcg_ctx *c, int sq, int ntq, const std::vector<int> &tkey, c
         op.nacc = nacc;
         op.nspin = h.nspin;
         op.sq = sq;
+        // the chunk's sources summed in FP32 shared-memory planes, one FP64
+        // red.add per accumulator point at the end (in place of one per source)
+        op.sacc_on = c->qp_sacc ? 1 : 0;
+        op.sacc_n = nacc;
         TRY((run_chunk<T, OQ>(c, op, (int)items, p.nt)));
     }
     return TCG_OK;

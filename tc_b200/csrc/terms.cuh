@@ -226,12 +226,16 @@ struct OpBase {
     // sources in SACC shared-memory planes per CTA (xyi_sterm picks the slot
     // of output b, -1 for none) and adds them to the FP64 accumulators once
     // at the end (xyi_sflush), instead of one FP64 red.add per source
-    static constexpr int SACC = 0;
-    int sacc_on = 0;                         // runtime switch of the SACC path (TCG_SACC turns it on; measured
-                                             // equal to the red.add path on the C3 workload, so off by default)
+    static constexpr int SACC = 0;           // most slots an op uses (compile-time bound)
+    int sacc_on = 0;                         // runtime switch of the SACC path
+    int sacc_n = 0;                          // slots in use when on (<= SACC; sizes the shared memory)
     __device__ int xyi_slot(int) const { return -1; }
     __device__ V xyi_sterm(int, int, int, size_t, V v) const { return v; }
     __device__ void xyi_sflush(int, int, size_t, V) const {}
+    // SACC_GROUP: the op defines xyi_sgroup(tj, item, b0, p, vals[GS], add),
+    // the contributions of an output group to the slots (add(slot, value));
+    // otherwise output b0 goes to slot xyi_slot(b0) as xyi_sterm (sacc_group)
+    static constexpr bool SACC_GROUP = false;
     __device__ bool regacc_grid(int) const { return false; }
     __device__ V xyi_term(int, int, int, size_t, const V *v) const { return v[0]; }
     __device__ void xyi_flush(int, size_t, V) const {}
@@ -695,6 +699,41 @@ struct OpQP : OpBase<T> {
         else { w = 0; xs = o / 3; d = o % 3; }
         if (EQ) xs = sq;
         return cscale(in[w], (S)(G[d] * tab[xs] * this->invN));   // du[x]_d * phiphi (:378, :385)
+    }
+    // shared-memory accumulation (k_xyi_t6, FP32): slot a = accumulator a of
+    // the target (3a2 per spin, 3a4_d, 3b5_d), the same sums as xyi_accum
+    static constexpr int SACC = 8;
+    static constexpr bool SACC_GROUP = true;
+    template <class F>
+    __device__ void xyi_sgroup(int, int item, int b, size_t p, const V *v, F &&add) const
+    {
+        using S = decltype(v[0].x);
+        const size_t N = this->g.N;
+        const int si = item % this->ns;
+        const S f1 = (S)fill[si];
+        int xs, d;
+        if (BITC) { xs = (b >> 1) / 3; d = (b >> 1) % 3; }
+        else { xs = b / 3; d = b % 3; }
+        if (EQ) xs = sq;
+        const V o1 = v[0];
+        V c3a2;
+        if constexpr (BITC) c3a2 = cmulc(v[1], o1);
+        else c3a2 = V{o1.x * o1.x + o1.y * o1.y, (S)0};
+        if (EQ) {
+            if (nspin == 1) add(0, cscale(c3a2, -2 * f1));
+            else { add(0, cscale(c3a2, -f1)); add(1, cscale(c3a2, -f1)); }
+        } else {
+            add(nspin == 1 ? 0 : xs, cscale(c3a2, -f1));
+        }
+        if (xs == sq) {
+            add(nspin + d, cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * N + p])), f1));
+            if constexpr (BITC)
+                add(nspin + 3 + d, cscale(cmul(cconj(v[1]), cconj(__ldg(&Rchi[(size_t)si * N + p]))), -f1));
+        }
+    }
+    __device__ void xyi_sflush(int tj, int slot, size_t p, V sum) const
+    {
+        acc_red(acc + ((size_t)tj * nacc + slot) * this->g.N + p, to64(sum), 1.0);
     }
     __device__ void xyi_accum(int tj, int item, int b, size_t p, const V *v) const
     {

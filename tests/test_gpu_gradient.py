@@ -104,3 +104,54 @@ def test_jastrow_table_gradient_fd():
         fd = (vals[0] - vals[1]) / (2 * H)
         print(f"d E2 / d {which}: adjoint {pred:.10e}, finite difference {fd:.10e}")
         assert abs(fd - pred) <= 1e-6 * max(abs(pred), 1e-6)
+
+
+def test_c4_gradients_fd():
+    """The adjoint at the homogeneous-electron-gas configuration C4 in full
+    (simple cubic, 54 electrons at r_s = 2, Gamma only, 27 occupied + 27 trial
+    bands, grid 40^3, TC++'s default RPA Jastrow): dE/d conj(chi) of all
+    terms along a seeded random direction of every occupied left orbital,
+    and the tc2x Jastrow-table gradient contracted with d u / d A, d V_2body /
+    d A, against central finite differences (h = 1e-5) of the FP64 energy."""
+    import torch
+    s = synth.heg_config()
+    mask = abi.TERMS_TC
+    with Context(s, "fp64") as ctx:
+        s.density = ctx.density()
+        ctx.set_state()
+        buf = torch.zeros(s.phik_left.size * 2, dtype=torch.float64, device="cuda")
+        ctx.energy_grad(mask, dchi_ptr=buf.data_ptr())
+        torch.cuda.synchronize()
+        grad = buf.cpu().numpy().view(np.complex128)
+    rng = np.random.default_rng(11)
+    delta = rng.standard_normal(grad.shape) + 1j * rng.standard_normal(grad.shape)
+    nb, no, npw = int(s.nbands[0]), int(s.nocc[0][0]), int(s.npw[0])
+    delta.reshape(nb, npw)[no:] = 0.0                  # occupied orbitals only
+    vals = []
+    for d in (H, -H):
+        t = copy.copy(s)
+        t.phik_left = s.phik_left + d * delta
+        vals.append(energy(t, mask))
+    fd = (vals[0] - vals[1]) / (2 * H)
+    pred = np.sum(grad * np.conj(delta))
+    print(f"C4 d E / d h along a random direction: adjoint {pred:.10e}, finite difference {fd:.10e}")
+    assert abs(fd - pred) <= 1e-6 * abs(pred)
+
+    A0, F0 = s.jastrow_A[0, 0], s.jastrow_F[0, 0]
+    with Context(s, "fp64") as ctx:
+        ctx.set_state()
+        _, _, du, dv = ctx.energy_grad(abi.TERM_TC2X, tables=True)
+    h = 1e-7
+    ua, va = _rpa_tables(s, A0 + 1j * h, F0)
+    pred = np.sum(du[0] * ua.imag / h) + np.sum(dv[0] * va.imag / h)
+    vals = []
+    for d in (H, -H):
+        t = copy.copy(s)
+        t.jastrow_A = s.jastrow_A + d                  # tc2x reads the same-spin channel only
+        with Context(t, "fp64") as ctx:
+            ctx.set_state()
+            e2, _, _, _ = ctx.energy_grad(abi.TERM_TC2X)
+        vals.append(e2)
+    fd = (vals[0] - vals[1]) / (2 * H)
+    print(f"C4 d E2 / d A: adjoint {pred:.10e}, finite difference {fd:.10e}")
+    assert abs(fd - pred) <= 1e-6 * max(abs(pred), 1e-6)

@@ -339,3 +339,23 @@ def test_36_pruned_transforms(monkeypatch, method, prune, prec, tol):
     assert rel(g2, r2) < tol
     if method != "HF":
         assert rel(g3, r3) < tol
+
+
+@pytest.mark.parametrize("method", ["TC", "BITC"])
+@pytest.mark.parametrize("sacc", ["qp-default", "qp-off", "3a3b6A-on"])
+def test_36_shared_memory_accumulation(monkeypatch, method, sacc):
+    """36^3 mixed precision: the inverse XY pass summing a chunk's sources in
+    FP32 shared-memory planes -- on by default for the occupied-pair stage of
+    tc3a2a4b2b5 (TCG_NO_QP_SACC turns it off), optional for the first stage
+    of tc3a3b3b4b6 (TCG_SACC) -- vs the oracle"""
+    if sacc == "qp-off":
+        monkeypatch.setenv("TCG_NO_QP_SACC", "1")
+    if sacc == "3a3b6A-on":
+        monkeypatch.setenv("TCG_SACC", "1")
+    s = system(method, nr=(36, 36, 36), nk=2, ecut=4.0, nbands=3, nocc=2)
+    for mask in (abi.TERM_TC3A2A4B2B5, abi.TERM_TC3A3B3B4B6):
+        _, r3 = oracle_terms(s, mask)
+        with Context(s, "mixed") as ctx:
+            ctx.set_state()
+            _, g3 = ctx.apply(mask)
+        assert rel(g3, r3) < MIXED_TOL
