@@ -64,7 +64,11 @@ class QEData:
         if mag.find("noncolin").text.strip() == "true":
             raise ValueError("non-collinear QE runs are outside this library's scope")
         band = out.find("band_structure")
-        self.nbnd = int(band.find("nbnd").text)
+        if self.lsda:
+            self.nbnd_s = [int(band.find("nbnd_up").text), int(band.find("nbnd_dw").text)]
+        else:
+            self.nbnd_s = [int(band.find("nbnd").text)]
+        self.nbnd = self.nbnd_s[0]
         self.nelec = float(band.find("nelec").text)
         self.kcart, self.kweight, self.npw_k, self.eig, self.occ = [], [], [], [], []
         for ks in band.findall("ks_energies"):
@@ -83,13 +87,26 @@ class QEData:
     _FIELDS = ("alat", "lattice", "recip_norm", "recip", "nr", "gamma_only", "rotation_qe", "translation", "noinv",
                "lsda", "nbnd", "nelec", "kcart", "kweight", "npw_k", "kcrys")
 
+    @property
+    def nspin(self):
+        return 2 if self.lsda else 1
+
+    def eig_spin(self, ik, s):
+        """Eigenvalues (Ha) of spin s at irreducible k: QE lists the up bands, then the down bands."""
+        o = sum(self.nbnd_s[:s])
+        return self.eig[ik][o:o + self.nbnd_s[s]]
+
     def save_npz(self, path):
         d = {f: np.asarray(getattr(self, f)) for f in self._FIELDS}
+        d["nbnd_s"] = np.array(self.nbnd_s)
         d["atom_names"] = np.array([n for n, _ in self.atoms])
         d["atom_pos"] = np.array([p for _, p in self.atoms])
         for ik in range(len(self.kweight)):
-            m, c = self.read_wfc(ik)
-            d[f"mill_{ik}"], d[f"evc_{ik}"], d[f"eig_{ik}"], d[f"occ_{ik}"] = m, c, self.eig[ik], self.occ[ik]
+            d[f"eig_{ik}"], d[f"occ_{ik}"] = self.eig[ik], self.occ[ik]
+            for sp in range(self.nspin):
+                m, c = self.read_wfc(ik, sp)
+                tag = "" if sp == 0 else "dw_"
+                d[f"mill_{tag}{ik}"], d[f"evc_{tag}{ik}"] = m, c
         np.savez_compressed(path, **d)
 
     @classmethod
@@ -107,14 +124,18 @@ class QEData:
         q.occ = [z[f"occ_{ik}"] for ik in range(nk)]
         q.atoms = [(str(n), p) for n, p in zip(z["atom_names"], z["atom_pos"])] if "atom_names" in z else []
         q.pseudo_files = {}
-        q._wfc = [(z[f"mill_{ik}"], z[f"evc_{ik}"]) for ik in range(nk)]
+        q.nbnd_s = [int(x) for x in z["nbnd_s"]] if "nbnd_s" in z else [int(q.nbnd)]
+        q._wfc = [[(z[f"mill_{tag}{ik}"], z[f"evc_{tag}{ik}"]) for ik in range(nk)]
+                  for tag in ([""] if not q.lsda else ["", "dw_"])]
         return q
 
-    def read_wfc(self, ik):
-        """(miller [npw][3] int, coefficients [nbnd][npw] complex) of wfc{ik+1}.dat_nonbin."""
+    def read_wfc(self, ik, spin=0):
+        """(miller [npw][3] int, coefficients [nbnd][npw] complex) of wfc{ik+1}.dat_nonbin
+        (wfcup / wfcdw for spin-polarised runs)."""
         if getattr(self, "_wfc", None) is not None:
-            return self._wfc[ik]
-        path = os.path.join(self.dir, f"wfc{ik + 1}.dat_nonbin")
+            return self._wfc[spin][ik]
+        name = f"wfc{ik + 1}" if not self.lsda else f"wfc{'up' if spin == 0 else 'dw'}{ik + 1}"
+        path = os.path.join(self.dir, f"{name}.dat_nonbin")
         with open(path) as f:
             lines = f.read().split("\n")
         h = lines[0].split()
@@ -186,28 +207,39 @@ def gindex_phase(mill, U, t, tr, nr):
 
 
 def system_from_qe(save_dir, method="BITC", A=None, F=None, nbands=None, nb_apply=None, name=None,
-                   includes_div_correction=True):
+                   includes_div_correction=True, smearing="fixed", smearing_width=0.01):
     """TCSystem of the first SCF iteration of a TC++ run on a QE save directory
-    (or a QEData, or the .npz written by QEData.save_npz):
-    the QE orbitals as right (and, for BITC, left) orbitals, fillings 2 (1 per spin
-    channel when spin-polarised) for the bands QE occupies, the density of these
-    orbitals, divergence sums of the SCF mesh.  A, F: 2x2 RPA Jastrow parameters."""
+    (or a QEData, or the .npz written by QEData.save_npz): the QE orbitals as
+    right (and, for BITC, left) orbitals, one spin channel per QE spin (lsda),
+    the occupations TC++'s set_filling gives the QE eigenvalues (smearing
+    "fixed" or "gaussian" with smearing_width in Ha; tc_b200.occupations),
+    the density of these orbitals, divergence sums of the SCF mesh.
+    A, F: 2x2 RPA Jastrow parameters."""
     from . import synth
+    from .occupations import fermi_filling, occupied_counts
     q = save_dir if isinstance(save_dir, QEData) else (
         QEData.load_npz(save_dir) if str(save_dir).endswith(".npz") else QEData(save_dir))
     if q.gamma_only:
         raise ValueError("gamma_only QE runs are not supported here")
-    if q.lsda:
-        raise ValueError("spin-polarised QE runs are not supported by this reader")
+    nspin = q.nspin
     nr = q.nr
+    if min(q.kweight) < 1e-8:
+        raise ValueError("k-points of zero weight (whose divergence corrections need the kVaux sums of BAND-mode "
+                         "runs) are outside this library's scope")
     U = tc_rotations(q.rotation_qe)
     star = expand_kpoints(q.kcrys, q.kweight, U, not q.noinv)
     nk = len(star)
-    nbnd = q.nbnd if nbands is None else int(nbands)
+    nbnd = min(q.nbnd_s) if nbands is None else int(nbands)
+    if nbnd > min(q.nbnd_s):
+        raise ValueError("more bands requested than the QE run has")
+    eig = np.array([[q.eig_spin(ik, sp)[:nbnd] for ik in range(nk)] for sp in range(nspin)])
+    fill, _ = fermi_filling(eig, q.kweight, q.nelec, nspin, smearing, smearing_width)
+    nocc = occupied_counts(fill)
     kvec_all, time_rev, rot_index, nsym_k = [], [], [], []
-    gidx, phase, phik, npw, nocc, fill = [], [], [], [], [], []
+    gidx, phase, npw = [], [], []
+    phik = [[None] * nk for _ in range(nspin)]
     for ik in range(nk):
-        mill, c = q.read_wfc(ik)
+        mill, _ = q.read_wfc(ik, 0)
         mill = wrap_miller(mill, nr)
         npw.append(len(mill))
         nsym_k.append(len(star[ik]))
@@ -218,10 +250,11 @@ def system_from_qe(save_dir, method="BITC", A=None, F=None, nbands=None, nb_appl
             gi, ph = gindex_phase(mill, U[isym], q.translation[isym], tr, nr)
             gidx.append(gi)
             phase.append(ph)
-        phik.append(c[:nbnd])
-        occ = q.occ[ik][:nbnd]
-        nocc.append(int(np.sum(occ > 1e-8)))
-        fill.append(np.where(occ > 1e-8, 2.0, 0.0))
+        for sp in range(nspin):
+            m2, c = q.read_wfc(ik, sp)
+            if not np.array_equal(wrap_miller(m2, nr), mill):
+                raise ValueError("the spin channels of a k-point have different plane-wave sets")
+            phik[sp][ik] = c[:nbnd]
     lattice = q.lattice
     recip = q.recip
     omega = abs(float(np.linalg.det(lattice)))
@@ -231,22 +264,26 @@ def system_from_qe(save_dir, method="BITC", A=None, F=None, nbands=None, nb_appl
         A = np.zeros((2, 2)) if method == "HF" else None
     Aarr = np.asarray(A, dtype=np.float64) if A is not None else np.zeros((2, 2))
     Farr = np.asarray(F, dtype=np.float64) if F is not None else np.ones((2, 2))
-    flat = np.concatenate([np.ascontiguousarray(P).ravel() for P in phik])
+    flat = np.concatenate([np.ascontiguousarray(P).ravel() for sp in range(nspin) for P in phik[sp]])
     s = TCSystem(
-        nr=nr, recip=recip, lattice=lattice, omega=omega, method=method, nspin=1,
+        nr=nr, recip=recip, lattice=lattice, omega=omega, method=method, nspin=nspin,
         nsym_k=np.array(nsym_k, dtype=np.int32), kvec=kvec_all, time_rev=np.array(time_rev, dtype=np.uint8),
         rot_index=np.array(rot_index, dtype=np.int32), rotation=U.astype(np.int32),
         translation=np.asarray(q.translation, dtype=np.float64), num_kpoints=int(len(kvec_all)),
-        npw=np.array(npw, dtype=np.int32), gindex=np.concatenate(gidx).astype(np.int32),
-        phase=np.concatenate(phase), jastrow_A=Aarr, jastrow_F=Farr,
+        npw=np.array(npw, dtype=np.int32), gindex=np.concatenate(gidx * nspin).astype(np.int32),
+        phase=np.concatenate(phase * nspin), jastrow_A=Aarr, jastrow_F=Farr,
         includes_div_correction=includes_div_correction, alpha_Vaux=float(alpha), sum_Vaux=sumv,
-        nbands=np.array([nbnd], dtype=np.int32), nocc=np.array([nocc], dtype=np.int32),
-        filling=np.concatenate(fill), phik=flat, phik_left=flat.copy() if method == "BITC" else None,
+        nbands=np.full(nspin, nbnd, dtype=np.int32), nocc=nocc,
+        filling=fill.ravel(), phik=flat, phik_left=flat.copy() if method == "BITC" else None,
         density=np.zeros((2, int(np.prod(nr))), dtype=np.complex128), name=name or "qe",
     )
     s.density = synth.density_numpy(s)
     nb = nbnd if nb_apply is None else int(nb_apply)
-    s.nb_apply = np.full((1, nk), nb, dtype=np.int32)
-    s.psi = np.concatenate([np.ascontiguousarray(P[:nb]).ravel() for P in phik])
+    s.nb_apply = np.full((nspin, nk), nb, dtype=np.int32)
+    s.psi = np.concatenate([np.ascontiguousarray(P[:nb]).ravel() for sp in range(nspin) for P in phik[sp]])
     s.meta["qe"] = q
+    s.meta["kweight"] = np.asarray(q.kweight, dtype=np.float64)
+    s.meta["nelec"] = float(q.nelec)
+    s.meta["eig"] = eig
+    s.meta["smearing"] = (smearing, float(smearing_width))
     return s

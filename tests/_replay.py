@@ -39,21 +39,20 @@ def examples():
 
 
 def si_system(example):
-    """(TCSystem of the first SCF iteration, Pseudo, QE eigenvalues [nk][nb],
-    golden record) of one of test/example{1,2,3}."""
+    """(TCSystem of the first SCF iteration, Pseudo, QE eigenvalues
+    [nspin][nk][nb], golden record) of one of the replayed runs."""
     rec = examples()[example]
     method = rec["calc_method"]
-    q = QEData.load_npz(os.path.join(GOLDEN, "qe_si.npz"))
+    q = QEData.load_npz(os.path.join(GOLDEN, rec["qe"]))
     A = F = None
     if "F" in rec:
         F = np.array(rec["F"], dtype=np.float64)
         A = np.array([[F[0, 0] ** 2 / 2, F[0, 1] ** 2], [F[1, 0] ** 2, F[1, 1] ** 2 / 2]])
-    s = system_from_qe(q, method=method, A=A, F=F)
+    s = system_from_qe(q, method=method, A=A, F=F, smearing=rec["smearing"], smearing_width=rec["smearing_width"])
     upf = UPF.from_arrays(np.load(os.path.join(GOLDEN, "si_upf.npz")))
     sp, pos, _ = species_and_positions(q)
     pp = pseudo_from_upf(s, [upf], sp, pos)
-    eig = [np.asarray(e[:int(s.nbands[0])], dtype=np.float64) for e in q.eig]
-    return s, pp, eig, rec
+    return s, pp, s.meta["eig"], rec
 
 
 def kg2(system, k):
@@ -100,124 +99,137 @@ def sort_eigen(w, X):
 
 def davidson(system, apply, eig_ref, max_blocks=2):
     """One Diagonalization::block_davidson call (num_refresh_david 1, not
-    bi-orthogonal).  apply(psi_flat, nb_apply[1][nk]) -> (h1, h2, h3) flat,
-    packed like psi.  Returns eigenvalues [nk][nb] and energies e[n][nk][nb]
-    (n = 1-, 2-, 3-body: diag(L^H H_n,sub X), L = (X^-1)^H for BITC)."""
+    bi-orthogonal) for every spin channel.  apply(psi_flat, nb_apply[nspin][nk])
+    -> (h1, h2, h3) flat, packed like psi.  eig_ref [nspin][nk][nb]: the
+    previous eigenvalues.  Returns eigenvalues [nspin][nk][nb] and energies
+    e[n][nspin][nk][nb] (n = 1-, 2-, 3-body: diag(L^H H_n,sub X),
+    L = (X^-1)^H for BITC); the new orbitals stay in davidson.last_orbitals."""
     bitc = system.method == "BITC"
-    nk = system.nk_irr
+    ns, nk = system.nspin, system.nk_irr
     nb = int(system.nbands[0])
-    V = []
-    for k in range(nk):
-        rows = [system.orb(0, k, b).copy() for b in range(nb)]
-        if bitc:                                             # :64-71
-            out = []
-            for r in rows:
-                g = gram_schmidt(out, r)
-                assert g is not None
-                out.append(g)
-            rows = out
-        V.append(rows)
-    HV = [[[] for _ in range(nk)] for _ in range(3)]
-    nfix = [0] * nk
+    V = {}
+    for sp in range(ns):
+        for k in range(nk):
+            rows = [system.orb(sp, k, b).copy() for b in range(nb)]
+            if bitc:                                             # :64-71
+                out = []
+                for r in rows:
+                    g = gram_schmidt(out, r)
+                    assert g is not None
+                    out.append(g)
+                rows = out
+            V[sp, k] = rows
+    HV = {key: [[], [], []] for key in V}
+    nfix = {key: 0 for key in V}
+    keys = [(sp, k) for sp in range(ns) for k in range(nk)]
 
     def run_block():
-        blocks = [V[k][nfix[k]:] for k in range(nk)]
-        nba = np.array([[len(b) for b in blocks]], dtype=np.int32)
-        psi = np.concatenate([np.concatenate(b) for b in blocks])
+        blocks = {key: V[key][nfix[key]:] for key in keys}
+        nba = np.array([[len(blocks[sp, k]) for k in range(nk)] for sp in range(ns)], dtype=np.int32)
+        psi = np.concatenate([np.concatenate(blocks[key]) for key in keys])
         hs = apply(psi, nba)
         off = 0
-        out = []
-        for k in range(nk):
-            npw = len(V[k][0])
+        out = {}
+        for key in keys:
+            npw = len(V[key][0])
             per = []
-            for i in range(len(blocks[k])):
+            for i in range(len(blocks[key])):
                 sl = slice(off, off + npw)
                 per.append(tuple(None if h is None else h[sl].copy() for h in hs))
                 off += npw
-            out.append(per)
+            out[key] = per
         return blocks, out
 
     for _ in range(max_blocks - 1):                                  # :207-400
         blocks, hs = run_block()
-        for k in range(nk):
-            kG2 = kg2(system, k)
-            old = len(V[k])
-            for i, phi in enumerate(blocks[k]):
-                h1, h2, h3 = hs[k][i]
+        for key in keys:
+            kG2 = kg2(system, key[1])
+            old = len(V[key])
+            for i, phi in enumerate(blocks[key]):
+                h1, h2, h3 = hs[key][i]
                 for n, h in enumerate((h1, h2, h3)):
-                    HV[n][k].append(h)
+                    HV[key][n].append(h)
                 htot = sum(h for h in (h1, h2, h3) if h is not None)
-                t = precondition(kG2, phi, htot, eig_ref[k][i])
-                g = gram_schmidt(V[k], t)
+                t = precondition(kG2, phi, htot, eig_ref[key[0]][key[1]][i])
+                g = gram_schmidt(V[key], t)
                 if g is not None:
-                    V[k].append(g)
-            nfix[k] = old
+                    V[key].append(g)
+            nfix[key] = old
     blocks, hs = run_block()                                          # :405-430
-    for k in range(nk):
-        for i in range(len(blocks[k])):
+    for key in keys:
+        for i in range(len(blocks[key])):
             for n in range(3):
-                HV[n][k].append(hs[k][i][n])
-    eig = np.zeros((nk, nb), dtype=np.complex128)
-    en = np.zeros((3, nk, nb), dtype=np.complex128)
-    right, left = [], []
-    for k in range(nk):                                               # :431-600
-        Vm = np.array(V[k])
-        Hn = [None if HV[n][k][0] is None else Vm.conj() @ np.array(HV[n][k]).T for n in range(3)]
+                HV[key][n].append(hs[key][i][n])
+    eig = np.zeros((ns, nk, nb), dtype=np.complex128)
+    en = np.zeros((3, ns, nk, nb), dtype=np.complex128)
+    right, left = {}, {}
+    for key in keys:                                                  # :431-600
+        sp, k = key
+        Vm = np.array(V[key])
+        Hn = [None if HV[key][n][0] is None else Vm.conj() @ np.array(HV[key][n]).T for n in range(3)]
         H = sum(h for h in Hn if h is not None)
         w, X = np.linalg.eig(H)
         w, X = sort_eigen(w, X)
         L = np.linalg.inv(X).conj().T if bitc else X
-        eig[k] = w[:nb]
+        eig[sp, k] = w[:nb]
         for n in range(3):
             if Hn[n] is not None:
-                en[n, k] = np.einsum("ai,ab,bi->i", L[:, :nb].conj(), Hn[n], X[:, :nb])
+                en[n, sp, k] = np.einsum("ai,ab,bi->i", L[:, :nb].conj(), Hn[n], X[:, :nb])
         R = X[:, :nb].T @ Vm                                          # V X
         if bitc:                                                      # BITC final loop: V X, V (X^-1)^H
-            right.append(R)
-            left.append(L[:, :nb].T @ Vm)
+            right[key] = R
+            left[key] = L[:, :nb].T @ Vm
         else:                                                         # Gram-Schmidt of V X
             out = []
             for r in R:
                 g = gram_schmidt(out, r)
                 assert g is not None
                 out.append(g)
-            right.append(np.array(out))
-    davidson.last_orbitals = (right, left if bitc else None)
+            right[key] = np.array(out)
+    davidson.last_orbitals = ([right[key] for key in keys], [left[key] for key in keys] if bitc else None)
     return eig, en
 
 
-def scf_update(system, eig, nelec, mixing_beta=0.7):
+def occupations(system, eig):
+    """set_filling with the run's smearing on eigenvalues [nspin][nk][nb]."""
+    from tc_b200.occupations import fermi_filling
+    mode, width = system.meta["smearing"]
+    f, _ = fermi_filling(eig, system.meta["kweight"], system.meta["nelec"], system.nspin, mode, width)
+    return f
+
+
+def scf_update(system, eig, mixing_beta=0.7):
     """Next SCF iteration's system from the last davidson() call: new
-    orbitals, fixed occupations, density of the new orbitals (numpy
-    restatement of set_density) mixed with the previous one,
+    orbitals, occupations of the new eigenvalues, density of the new orbitals
+    (numpy restatement of set_density) mixed with the previous one,
     (1 - beta) n_old + beta n_new (bloch_states_scfloop_filling_density.cpp:340-345)."""
     import dataclasses
     from tc_b200 import synth
+    from tc_b200.occupations import occupied_counts
     right, left = davidson.last_orbitals
-    nocc = int(round(nelec / 2.0))
-    nb = int(system.nbands[0])
-    f = np.zeros((system.nk_irr, nb))
-    f[:, :nocc] = 2.0
+    f = occupations(system, eig)
     s = dataclasses.replace(system, phik=np.concatenate([r.ravel() for r in right]),
                             phik_left=None if left is None else np.concatenate([l.ravel() for l in left]),
-                            filling=f.ravel(), nocc=np.full((1, system.nk_irr), nocc, dtype=np.int32),
-                            meta=dict(system.meta))
+                            filling=f.ravel(), nocc=occupied_counts(f), meta=dict(system.meta))
     s.density = (1.0 - mixing_beta) * system.density + mixing_beta * synth.density_numpy(s)
     return s
 
 
-def total_energy(system, eig, en, nelec):
-    """(E_1, E_2, E_3) with fixed occupations: f = 2 for the nelec/2 lowest bands."""
-    nocc = int(round(nelec / 2.0))
+def total_energy(system, eig, en):
+    """(E_1, E_2, E_3) with the occupations of the new eigenvalues
+    (calc_total_energy runs after set_filling of the next iteration)."""
+    f = occupations(system, eig)
     E = np.zeros(3, dtype=np.complex128)
     w = np.array([1.0, 0.5, 1.0 / 3.0])
-    for k in range(system.nk_irr):
-        a0 = int(system.kall_off[k])
-        for isym in range(int(system.nsym_k[k])):
-            tr = bool(system.time_rev[a0 + isym])
-            for b in range(nocc):
-                e = np.conj(en[:, k, b]) if tr else en[:, k, b]
-                E += 2.0 * w * e
+    for sp in range(system.nspin):
+        for k in range(system.nk_irr):
+            if system.meta["kweight"][k] < 1e-8:
+                continue
+            a0 = int(system.kall_off[k])
+            for isym in range(int(system.nsym_k[k])):
+                tr = bool(system.time_rev[a0 + isym])
+                e = np.conj(en[:, sp, k]) if tr else en[:, sp, k]
+                E += (e * f[sp, k][None, :]).sum(axis=1) * w
     return E / system.num_kpoints
 
 

@@ -1,12 +1,21 @@
 """Generate the fixtures of the golden-replay tests from the reference's test
-data test/example1 (HF), test/example2 (TC) and test/example3 (BITC): fcc Si,
-16^3 grid, 6 bands, 3 irreducible k-points expanded to 8 by symmetry, all
-three starting from the same Quantum ESPRESSO files.
+data: fcc Si, 16^3 grid, 6 bands per spin, from two Quantum ESPRESSO runs,
+each replayed with HF, TC and BITC:
 
-  qe_si.npz        the QE data TC++ reads (tc_b200.qe.QEData.save_npz, with atoms)
-  si_upf.npz       the arrays TC++ reads from Si_test.upf (tc_b200.upf.UPF)
-  si_examples.json per example: calc_method, the RPA F of parameters.casl, and
-                   the energies TC++ printed after SCF iterations 1 and 2
+  test/example1-3    3 irreducible k-points (8 by symmetry), fixed occupations
+  test/example17-19  spin-polarised (lsda), 3 irreducible k-points, Gaussian smearing (0.1 Ha)
+
+(test/example10-12 add two k-points of zero weight, whose divergence
+corrections take the kVaux sums of BAND-mode runs; those are outside this
+library's scope, so they are not replayed.)
+
+  qe_si.npz, qe_si_lsda.npz
+                   the QE data TC++ reads (tc_b200.qe.QEData.save_npz, with atoms)
+  si_upf.npz       the arrays TC++ reads from Si_test.upf (tc_b200.upf.UPF;
+                   every example uses the same file)
+  si_examples.json per example: calc_method, its QE fixture, smearing mode and
+                   width (input.in), the RPA F of parameters.casl, and the
+                   energies TC++ printed after SCF iterations 1 and 2
                    ("Total energy (1-body terms)" and so on, output.out), with
                    the orbital energies (eV) printed after iteration 1
 
@@ -27,7 +36,19 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from tc_b200.qe import QEData  # noqa: E402
 from tc_b200.upf import read_casl_rpa, read_upf  # noqa: E402
 
-EXAMPLES = {"example1": "HF", "example2": "TC", "example3": "BITC"}
+QE_SETS = {"qe_si.npz": "example1", "qe_si_lsda.npz": "example17"}
+EXAMPLES = {"example1": "qe_si.npz", "example2": "qe_si.npz", "example3": "qe_si.npz",
+            "example17": "qe_si_lsda.npz", "example18": "qe_si_lsda.npz", "example19": "qe_si_lsda.npz"}
+
+
+def parse_input(path):
+    """calc_method, smearing mode and width (TC++ defaults: fixed, 0.01 Ha)."""
+    opts = {}
+    for line in open(path):
+        w = line.split()
+        if len(w) >= 2:
+            opts[w[0]] = w[1]
+    return opts["calc_method"], opts.get("smearing_mode", "fixed"), float(opts.get("smearing_width", 0.01))
 
 
 def parse_output(path):
@@ -56,17 +77,20 @@ def parse_output(path):
 
 
 def main(test_dir):
-    q = QEData(os.path.join(test_dir, "example1"))
-    q.save_npz(os.path.join(HERE, "qe_si.npz"))
+    for fname, ex in QE_SETS.items():
+        QEData(os.path.join(test_dir, ex)).save_npz(os.path.join(HERE, fname))
     upf = read_upf(os.path.join(test_dir, "example1", "Si_test.upf"))
     np.savez_compressed(os.path.join(HERE, "si_upf.npz"), **upf.arrays())
     out = {}
-    for ex, method in EXAMPLES.items():
+    for ex, qe in EXAMPLES.items():
         d = os.path.join(test_dir, ex)
-        rec = {"calc_method": method, "iterations": parse_output(os.path.join(d, "output.out"))}
+        method, smearing, width = parse_input(os.path.join(d, "input.in"))
+        rec = {"calc_method": method, "qe": qe, "smearing": smearing, "smearing_width": width,
+               "iterations": parse_output(os.path.join(d, "output.out"))}
         casl = os.path.join(d, "parameters.casl")
         if os.path.exists(casl):
-            rec["F"] = read_casl_rpa(casl)[1].tolist()
+            nspin = 2 if "lsda" in qe else 1
+            rec["F"] = read_casl_rpa(casl, nspin=nspin)[1].tolist()
         out[ex] = rec
     with open(os.path.join(HERE, "si_examples.json"), "w") as f:
         json.dump(out, f, indent=1)

@@ -1,7 +1,8 @@
 """The reference's own test runs replayed through the library on the GPU
-(test/example1 HF, test/example2 TC, test/example3 BITC; fcc Si with 48
-space-group operations, see tests/test_golden_replay.py for the CPU replay
-with the oracle that pins it):
+(test/example1-3 HF, TC, BITC with fixed occupations; test/example17-19 the
+same spin-polarised with Gaussian smearing; fcc Si with 48 space-group
+operations, see tests/test_golden_replay.py for the CPU replay with the
+oracle that pins it):
 
 - H phi from the CUDA path (all terms of each method, one-body terms with the
   Si_test.upf pseudopotential) inside the numpy restatement of the Davidson
@@ -23,7 +24,7 @@ pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-8
 MIXED_TOL = 1e-6
-EXAMPLES = ["example1", "example2", "example3"]
+EXAMPLES = list(R.examples())
 
 
 def gpu_apply(ctx, system):
@@ -58,11 +59,11 @@ def test_library_h_in_reference_scf(example, prec, tol):
     s, pp, eig, rec = R.si_system(example)
     with context(s, pp, prec) as ctx:
         e, en = R.davidson(s, gpu_apply(ctx, s), eig)
-    check(R.total_energy(s, e, en, nelec=8.0), rec["iterations"][0], tol, s.method)
-    s2 = R.scf_update(s, e, nelec=8.0)
+    check(R.total_energy(s, e, en), rec["iterations"][0], tol, s.method)
+    s2 = R.scf_update(s, e)
     with context(s2, pp, prec) as ctx:
         e2, en2 = R.davidson(s2, gpu_apply(ctx, s2), e)
-    check(R.total_energy(s2, e2, en2, nelec=8.0), rec["iterations"][1], tol, s.method)
+    check(R.total_energy(s2, e2, en2), rec["iterations"][1], tol, s.method)
 
 
 @pytest.mark.parametrize("example", EXAMPLES)
@@ -71,10 +72,10 @@ def test_device_davidson_two_scf_iterations(example):
     ref_e, _ = R.davidson(s, R.oracle_apply(s, pp), eig)
     with context(s, pp, "fp64") as ctx:
         res = davidson.block_davidson(ctx, s, eig)
-        check(davidson.total_energy(s, res, nelec=8.0), rec["iterations"][0], FP64_TOL, s.method)
+        check(davidson.total_energy(s, res), rec["iterations"][0], FP64_TOL, s.method)
         assert np.abs(res.eigenvalues - ref_e).max() <= 1e-9
-        assert res.basis_size == [2 * int(s.nbands[0])] * s.nk_irr
-        s2, eig2 = davidson.scf_update(ctx, s, res, nelec=8.0)
+        assert res.basis_size == [2 * int(s.nbands[0])] * (s.nspin * s.nk_irr)
+        s2, eig2 = davidson.scf_update(ctx, s, res)
     with context(s2, pp, "fp64") as ctx:
         res2 = davidson.block_davidson(ctx, s2, eig2)
-    check(davidson.total_energy(s2, res2, nelec=8.0), rec["iterations"][1], FP64_TOL, s.method)
+    check(davidson.total_energy(s2, res2), rec["iterations"][1], FP64_TOL, s.method)
