@@ -206,6 +206,22 @@ def gindex_phase(mill, U, t, tr, nr):
     return gi, ph
 
 
+def _wfc_full(q, ik, spin):
+    """Miller indices and coefficients of all plane waves of k: for a
+    gamma_only run QE stores half of them, and the -G partners follow the
+    stored list in its order, G = 0 skipped, with c(-G) = conj(c(G))
+    (PlaneWaveBasis::set_G_from_mill, plane_wave_basis.cpp:8-43;
+    BlochStates::set_phik_qe, bloch_states_initialize.cpp:215-265)."""
+    mill, c = q.read_wfc(ik, spin)
+    if not q.gamma_only:
+        return mill, c
+    zero = np.flatnonzero(np.all(mill == 0, axis=1))
+    if zero.size != 1:
+        raise ValueError("G = 0 not found in a gamma_only wave function")
+    rest = np.delete(np.arange(len(mill)), zero[0])
+    return np.concatenate([mill, -mill[rest]]), np.concatenate([c, np.conj(c[:, rest])], axis=1)
+
+
 def system_from_qe(save_dir, method="BITC", A=None, F=None, nbands=None, nb_apply=None, name=None,
                    includes_div_correction=True, smearing="fixed", smearing_width=0.01):
     """TCSystem of the first SCF iteration of a TC++ run on a QE save directory
@@ -219,8 +235,6 @@ def system_from_qe(save_dir, method="BITC", A=None, F=None, nbands=None, nb_appl
     from .occupations import fermi_filling, occupied_counts
     q = save_dir if isinstance(save_dir, QEData) else (
         QEData.load_npz(save_dir) if str(save_dir).endswith(".npz") else QEData(save_dir))
-    if q.gamma_only:
-        raise ValueError("gamma_only QE runs are not supported here")
     nspin = q.nspin
     nr = q.nr
     if min(q.kweight) < 1e-8:
@@ -239,7 +253,7 @@ def system_from_qe(save_dir, method="BITC", A=None, F=None, nbands=None, nb_appl
     gidx, phase, npw = [], [], []
     phik = [[None] * nk for _ in range(nspin)]
     for ik in range(nk):
-        mill, _ = q.read_wfc(ik, 0)
+        mill, _ = _wfc_full(q, ik, 0)
         mill = wrap_miller(mill, nr)
         npw.append(len(mill))
         nsym_k.append(len(star[ik]))
@@ -251,7 +265,7 @@ def system_from_qe(save_dir, method="BITC", A=None, F=None, nbands=None, nb_appl
             gidx.append(gi)
             phase.append(ph)
         for sp in range(nspin):
-            m2, c = q.read_wfc(ik, sp)
+            m2, c = _wfc_full(q, ik, sp)
             if not np.array_equal(wrap_miller(m2, nr), mill):
                 raise ValueError("the spin channels of a k-point have different plane-wave sets")
             phik[sp][ik] = c[:nbnd]

@@ -4,12 +4,16 @@ each replayed with HF, TC and BITC:
 
   test/example1-3    3 irreducible k-points (8 by symmetry), fixed occupations
   test/example17-19  spin-polarised (lsda), 3 irreducible k-points, Gaussian smearing (0.1 Ha)
+and two Gamma-only QE runs (half of the plane waves stored, 20^3 grid: the
+library's runtime-size FFT path) replayed with HF:
+  test/example26     unpolarised, fixed occupations
+  test/example27     spin-polarised, fixed occupations
 
 (test/example10-12 add two k-points of zero weight, whose divergence
 corrections take the kVaux sums of BAND-mode runs; those are outside this
 library's scope, so they are not replayed.)
 
-  qe_si.npz, qe_si_lsda.npz
+  qe_si.npz, qe_si_lsda.npz, qe_si_gamma.npz, qe_si_gamma_lsda.npz
                    the QE data TC++ reads (tc_b200.qe.QEData.save_npz, with atoms)
   si_upf.npz       the arrays TC++ reads from Si_test.upf (tc_b200.upf.UPF;
                    every example uses the same file)
@@ -36,9 +40,11 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from tc_b200.qe import QEData  # noqa: E402
 from tc_b200.upf import read_casl_rpa, read_upf  # noqa: E402
 
-QE_SETS = {"qe_si.npz": "example1", "qe_si_lsda.npz": "example17"}
+QE_SETS = {"qe_si.npz": "example1", "qe_si_lsda.npz": "example17", "qe_si_gamma.npz": "example26",
+           "qe_si_gamma_lsda.npz": "example27"}
 EXAMPLES = {"example1": "qe_si.npz", "example2": "qe_si.npz", "example3": "qe_si.npz",
-            "example17": "qe_si_lsda.npz", "example18": "qe_si_lsda.npz", "example19": "qe_si_lsda.npz"}
+            "example17": "qe_si_lsda.npz", "example18": "qe_si_lsda.npz", "example19": "qe_si_lsda.npz",
+            "example26": "qe_si_gamma.npz", "example27": "qe_si_gamma_lsda.npz"}
 
 
 def parse_input(path):
