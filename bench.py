@@ -40,6 +40,8 @@ WORKLOADS = {
           "grid 36^3, 16 bands/k (4 occ), all 5 TC terms + per-state work",
     "C3s": "BITC batched apply, profiling case: fcc Si a=10.26, 2x2x2 MP (8 k), 14 Ha, "
            "grid 36^3, 16 bands/k (4 occ), all 5 TC terms + per-state work",
+    "C5": "TC large-cell apply: simple-cubic Si8 a=10.26, 3x3x3 MP (27 k), 20 Ha (4590-4625 PW/k), "
+          "grid 48^3, 48 bands/k (16 occ), all 5 TC terms + per-state work",
 }
 
 
