@@ -299,6 +299,7 @@ extern "C" int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg
     if (getenv("TCG_NO_PRUNE")) c->no_prune = true;
     if (getenv("TCG_SACC")) c->use_sacc = true;
     if (getenv("TCG_NO_QP_SACC")) c->qp_sacc = false;
+    if (getenv("TCG_NO_FUSE")) c->no_fuse = true;
     if (c->fast_n == 36 && (rc = build_prune_table(c)) != TCG_OK) {
         tcg_ctx_destroy(c);
         return rc;

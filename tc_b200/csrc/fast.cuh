@@ -436,6 +436,7 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2)
                         for (int yy = 0; yy < N; yy++) {
                             V vals[1] = {v[yy]};
                             racc[yy] = cadd(racc[yy], op.xyi_term(tj, item, b0, (size_t)z * N * N + (size_t)yy * N + ln, vals));
+                            if constexpr (Op::RACC_EXTRA) op.xyi_extra(tj, item, b0, (size_t)z * N * N + (size_t)yy * N + ln, vals);
                         }
                     } else {
 #pragma unroll
@@ -571,6 +572,7 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2)
                 for (int yy = 0; yy < N; yy++) {
                     V vals[1] = {v[yy]};
                     racc[yy] = cadd(racc[yy], op.xyi_term(tj, item, b0, (size_t)z * N * N + (size_t)yy * N + ln, vals));
+                    if constexpr (Op::RACC_EXTRA) op.xyi_extra(tj, item, b0, (size_t)z * N * N + (size_t)yy * N + ln, vals);
                 }
             } else {
 #pragma unroll
@@ -746,7 +748,6 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
     constexpr int SA = sizeof(V) == 8 ? Op::SACC : 0;    // shared-memory accumulator planes (FP32)
     const bool sa_on = SA > 0 && op.sacc_on;
     const int nsa = sa_on ? op.sacc_n : 0;                // planes in use
-    static_assert(!(RACC && Op::REFWD), "re-forwarded outputs accumulate through xyi_accum");
     static_assert(!(Op::REFWD && Op::GS > 1), "re-forward needs GS == 1");
     static_assert(!(SA > 0 && RACC), "shared-memory accumulation replaces the register form");
     static_assert(!(SA > 0 && Op::GS > 1 && !Op::SACC_GROUP), "grouped outputs need the op's xyi_sgroup");
@@ -822,6 +823,7 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
             for (int k2 = 0; k2 < R; k2++) {
                 V vals[1] = {v[k2]};
                 racc[k2] = cadd(racc[k2], op.xyi_term(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals));
+                if constexpr (Op::RACC_EXTRA) op.xyi_extra(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals);
             }
         } else {
 #pragma unroll
@@ -1182,6 +1184,7 @@ __global__ void __launch_bounds__(CfgP<N, sizeof(typename C2<T>::t)>::THREADS)
                             for (int i = 0; i < M; i++) {
                                 V vals[1] = {v[i]};
                                 racc[i] = cadd(racc[i], op.xyi_term(tj, item, b0, pz + (size_t)i * N, vals));
+                                if constexpr (Op::RACC_EXTRA) op.xyi_extra(tj, item, b0, pz + (size_t)i * N, vals);
                             }
                         } else {
 #pragma unroll

@@ -895,8 +895,86 @@ static int tc3_stage_ab(tcg_ctx *c, const Targets &Tg, const TRange &TR, const S
     return TCG_OK;
 }
 
+// tc2x together with stages A and B of tc3a3b3b4b6 for spin s with equal
+// Jastrow channels (OpTC2X3 + OpTC3B3 + OpTC3B): tc2x's sum goes to acc2 (the
+// H2 accumulator), 3a3 / 3b4's to qsum, 3b3 and 3b6 to acc (H3)
 template <typename T>
-static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, double2 *acc)
+static int tc2x_tc3_stage_ab(tcg_ctx *c, const TRange &TR, const Sources &S, int s, double b3, double b6,
+                             double2 *acc2, double2 *acc, double2 *qsum)
+{
+    using V = typename C2<T>::t;
+    using OX = OpTC2X3<T>;
+    using OY = OpTC3B3<T>;
+    using OB = OpTC3B<T, true>;
+    const Host &h = c->h;
+    const size_t N = h.N;
+    const bool bitc = h.method == TCG_METHOD_BITC;
+    const int nsl = OX::NB, n2 = OB::NF;
+    std::vector<ChunkPlan> plan;
+    TRY(plan_chunks(c, c->meta, TR.n, TR.key, TR.cartk, (int)S.key.size(), S.key, S.cartq,
+                    max_items_for(c, nsl + n2, sizeof(V)), min_targets(c), plan));
+    for (const ChunkPlan &p : plan) {
+        const size_t items = (size_t)p.nt * p.ns;
+        TRY(c->tmp.ensure(items * nsl * N * sizeof(V)));
+        TRY(c->tmp2.ensure(items * n2 * N * sizeof(V)));
+        TRY(gen_tables<T>(c, p, TAB_TC2X, s));
+        OX x;
+        op_common<T>(c, x, p, nsl, 2);
+        x.Rpsi = c->Rpsi.as<V>() + (size_t)(TR.t0 + p.t0) * N;
+        x.Rgpsi = c->Rgpsi.as<V>() + (size_t)(TR.t0 + p.t0) * 3 * N;
+        x.Rocc = c->Rocc.as<V>() + (S.base + p.s0) * N;
+        x.Rchi = (bitc ? c->Rchi.as<V>() : c->Rocc.as<V>()) + (S.base + p.s0) * N;
+        x.Rgrad = c->Rgrad.as<V>() + (S.base + p.s0) * 3 * N;
+        x.acc = acc2 + (size_t)(TR.t0 + p.t0) * N;
+        x.fill = c->occfill.as<double>() + S.base + p.s0;
+        x.densT = c->densT.as<V>() + 2 * N;
+        x.qsum = qsum + (size_t)(TR.t0 + p.t0) * 3 * N;
+        x.tmp2 = c->tmp2.as<V>();
+        TRY((run_chunk<T, OX>(c, x, (int)items, p.nt)));
+        OY y;
+        op_common<T>(c, y, p, nsl, 2);
+        y.Rpsi = x.Rpsi;
+        y.Rocc = x.Rocc;
+        y.Rchi = x.Rchi;
+        y.dnu = c->dnuT.as<V>() + (size_t)s * 3 * N;
+        y.acc = acc + (size_t)(TR.t0 + p.t0) * N;
+        y.fill = x.fill;
+        y.b3 = b3;
+        TRY((run_chunk<T, OY>(c, y, (int)items, p.nt)));
+        // 3b6B reads du from 3a3b6A's table layout (TAB_U_SX, one record for equal channels)
+        TRY(gen_tables<T>(c, p, TAB_U_SX, s, 1));
+        OB b;
+        op_common<T>(c, b, p, nsl, 2);
+        b.Rocc = x.Rocc;
+        b.acc = y.acc;
+        b.tmp2 = x.tmp2;
+        b.b6 = b6;
+        b.s = s;
+        TRY((run_chunk<T, OB>(c, b, (int)items, p.nt, false, true)));
+    }
+    return TCG_OK;
+}
+
+// equal Jastrow channels of spin s: u(G; 0, s) == u(G; 1, s)
+static bool eq_channels(const Host &h, int s)
+{
+    return h.A[0 * 2 + s] == h.A[1 * 2 + s] && h.F[0 * 2 + s] == h.F[1 * 2 + s];
+}
+
+// tc2x runs fused with tc3a3b3b4b6 (tc2x_tc3_stage_ab) when both are applied,
+// at 36^3 with the default kernel forms, equal channels for every spin
+static bool fuse_tc2x_tc3(const tcg_ctx *c, uint32_t mask)
+{
+    const Host &h = c->h;
+    if (c->no_fuse || !(mask & TCG_TERM_TC2X) || !(mask & TCG_TERM_TC3A3B3B4B6)) return false;
+    if (c->fast_n != 36 || c->force_generic || c->xy_kernels != 0 || c->z_kernels != 0) return false;
+    for (int s = 0; s < h.nspin; s++)
+        if (!eq_channels(h, s)) return false;
+    return true;
+}
+
+template <typename T>
+static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, double2 *acc, double2 *acc2_fused)
 {
     PhaseScope ps_(c, "ap:tc3");
     using V = typename C2<T>::t;
@@ -916,9 +994,10 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
         Sources S = sources_of(c, s);
         if (TR.n == 0) continue;
         const V *dnuT = c->dnuT.as<V>() + (size_t)s * 3 * N;
-        // stages A + B
-        const bool eq = h.A[0 * 2 + s] == h.A[1 * 2 + s] && h.F[0 * 2 + s] == h.F[1 * 2 + s];
-        if (eq) TRY((tc3_stage_ab<T, true>(c, Tg, TR, S, s, b3, b6, acc, qsum)));
+        // stages A + B (with tc2x when acc2_fused is given)
+        const bool eq = eq_channels(h, s);
+        if (acc2_fused) TRY((tc2x_tc3_stage_ab<T>(c, TR, S, s, b3, b6, acc2_fused, acc, qsum)));
+        else if (eq) TRY((tc3_stage_ab<T, true>(c, Tg, TR, S, s, b3, b6, acc, qsum)));
         else TRY((tc3_stage_ab<T, false>(c, Tg, TR, S, s, b3, b6, acc, qsum)));
         // 3a3: acc += a3 sum_d qsum_d dnu_d  (:629-641)
         TRY(launch(c, k_dot3<T>, dim3((unsigned)((N + 255) / 256), TR.n), dim3(256), 0, (int)N,
@@ -1534,17 +1613,20 @@ static int apply_impl(tcg_ctx *c, const ApplyArgs &A)
     // ---- two-body terms (H2): exchange (hf2x / tc2x) and Hartree (hf2h / tc2h)
     // accumulate in one R-space grid per band, scaled by the exchange
     // factor tbf; the Hartree terms' own factor 1/(N_k Omega) enters as a / tbf
+    // tc2x fused with tc3a3b3b4b6: its sum is made in the H3 block below and
+    // the H2 accumulator finalised after it
+    const bool fused = !(A.mask & TCG_TERM_HF2X) && fuse_tc2x_tc3(c, A.mask);
+    double tbf = 1.0 / (h.num_kpoints * h.omega);
+    const bool exch = (A.mask & (TCG_TERM_HF2X | TCG_TERM_TC2X)) != 0;
     if (A.mask & TCG_TERMS_H2) {
         TRY(c->acc2.ensure(nt * N * sizeof(double2)));
         TRY(launch(c, k_zero, dim3(pblocks), dim3(256), 0, c->acc2.as<double2>(), nt * N));
-        const bool exch = (A.mask & (TCG_TERM_HF2X | TCG_TERM_TC2X)) != 0;
-        double tbf = 1.0 / (h.num_kpoints * h.omega);
         if (A.mask & TCG_TERM_HF2X) {
             tbf = -4.0 * PI_D / (h.num_kpoints * h.omega);
             TRY(run_hf2x<T>(c, Tg, c->acc2.as<double2>()));
         } else if (A.mask & TCG_TERM_TC2X) {
             tbf = -1.0 / (h.num_kpoints * h.omega);
-            TRY(run_tc2x<T>(c, Tg, c->acc2.as<double2>()));
+            if (!fused) TRY(run_tc2x<T>(c, Tg, c->acc2.as<double2>()));
         }
         if (exch && h.nspin == 1) tbf /= 2.0;
         if (A.mask & (TCG_TERM_HF2H | TCG_TERM_TC2H)) {
@@ -1562,8 +1644,10 @@ static int apply_impl(tcg_ctx *c, const ApplyArgs &A)
                            c->acc2.as<double2>() + (size_t)TR.t0 * N));
             }
         }
-        TRY(finalize_acc(c, Tg, c->acc2.as<double2>(), A.h2, tbf));
-        if (exch) TRY(div_2x(c, Tg, A, A.h2));
+        if (!fused) {
+            TRY(finalize_acc(c, Tg, c->acc2.as<double2>(), A.h2, tbf));
+            if (exch) TRY(div_2x(c, Tg, A, A.h2));
+        }
     }
     // ---- three-body terms (H3)
     const uint32_t m3 = A.mask & ~TCG_TERMS_H2;
@@ -1601,8 +1685,13 @@ static int apply_impl(tcg_ctx *c, const ApplyArgs &A)
                            acc + (size_t)TR.t0 * N));
             }
         if (m3 & TCG_TERM_TC3A2A4B2B5) TRY(run_tc3a2a4b2b5_band<T>(c, Tg, acc));
-        if (m3 & TCG_TERM_TC3A3B3B4B6) TRY(run_tc3a3b3b4b6<T>(c, Tg, A, acc));
+        if (m3 & TCG_TERM_TC3A3B3B4B6)
+            TRY(run_tc3a3b3b4b6<T>(c, Tg, A, acc, fused ? c->acc2.as<double2>() : nullptr));
         TRY(finalize_acc(c, Tg, acc, A.h3, 1.0));
+    }
+    if (fused) {
+        TRY(finalize_acc(c, Tg, c->acc2.as<double2>(), A.h2, tbf));
+        if (exch) TRY(div_2x(c, Tg, A, A.h2));
     }
     TCG_CUDA(cudaStreamSynchronize(c->stream));
     return TCG_OK;

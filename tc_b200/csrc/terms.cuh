@@ -222,6 +222,10 @@ struct OpBase {
     // chunk with xyi_flush; the other grids go through xyi_accum.
     static constexpr bool REGACC = false;
     static constexpr bool BOUTER = false;    // one register accumulator per output grid (xyi_flush_b)
+    // RACC_EXTRA: besides the register sum, every output also goes to
+    // xyi_extra(tj, item, b, p, v) (other accumulators of the op)
+    static constexpr bool RACC_EXTRA = false;
+    __device__ void xyi_extra(int, int, int, size_t, const V *) const {}
     // 36^3 inverse XY pass (k_xyi_t6), FP32: SACC > 0 accumulates the chunk's
     // sources in SACC shared-memory planes per CTA (xyi_sterm picks the slot
     // of output b, -1 for none) and adds them to the FP64 accumulators once
@@ -762,6 +766,100 @@ struct OpQP : OpBase<T> {
                 acc_red(A + (size_t)(nspin + 3 + d) * N + p, cc, -f1);               // (:428-430)
             }
         }
+    }
+};
+
+// ----------------------------------------- tc2x fused with tc3a3b3b4b6 --
+// tc2x and the first q loop of tc3a3b3b4b6 run over the same (target kj,
+// source qi) pairs with the same pair density rho = conj(chi_qi) psi_kj.  With
+// equal Jastrow channels for the targets' spin the transforms
+// w_d = IFFT[rho G_d u(G; s, s)] are tc2x's 2b_x1 grids (tc2x.cpp:353-369) and,
+// times the filling, 3a3b6A's outputs 1-3 (tc3a3b3b4b6.cpp:305-349).  OpTC2X3
+// is tc2x with those three outputs also summed into qsum_d (3a3 / 3b4) and
+// re-forwarded times the density (3b6, for OpTC3B); OpTC3B3 is the remaining
+// 3b3 part of 3a3b6A (output 0 from the dnu inputs).  Per pair this is 12
+// transforms instead of 16.  Both read tc2x's coefficient tables (TAB_TC2X:
+// V_2body / N and G_d u(s, s) / N), which equal 3a3b6A's for equal channels.
+template <typename T>
+struct OpTC2X3 : OpTC2X<T> {
+    using V = typename C2<T>::t;
+    static constexpr const char *NAME = "2x3A";
+    static constexpr bool REFWD = true;
+    static constexpr bool RACC_EXTRA = true;
+    const V *densT;               // [N] n_0 + n_1 (compute precision)
+    double2 *qsum;                // [nt][3][N]
+    V *tmp2;                      // [items][3][N] re-forwarded grids
+    __device__ bool refwd_want(int b) const { return b > 0; }
+    __device__ V refwd_load(int, int item, int, size_t p, V v) const
+    {
+        const int si = item % this->ns;
+        return cscale(cmul(v, __ldg(&densT[p])), (decltype(v.x))this->fill[si]);   // f orbital * n (:332)
+    }
+    __device__ V *refwd_grid(int item, int b) const { return tmp2 + ((size_t)item * 3 + (b - 1)) * this->g.N; }
+    // qsum_d += f w_d phi_q (:305-328); tc2x's own sum goes through the registers
+    __device__ void xyi_extra(int tj, int item, int b, size_t p, const V *v) const
+    {
+        if (b == 0) return;
+        const size_t N = this->g.N;
+        const int si = item % this->ns;
+        acc_red(qsum + ((size_t)tj * 3 + (b - 1)) * N + p, to64(cmul(v[0], __ldg(&this->Rocc[(size_t)si * N + p]))),
+                this->fill[si]);
+    }
+    __device__ void xyi_accum(int tj, int item, int b, size_t p, const V *v) const
+    {
+        OpTC2X<T>::xyi_accum(tj, item, b, p, v);
+        xyi_extra(tj, item, b, p, v);
+    }
+};
+
+template <typename T>
+struct OpTC3B3 : OpBase<T> {
+    using V = typename C2<T>::t;
+    static constexpr const char *NAME = "3b3A";
+    static constexpr int NF = 3, NB = 1;     // dnu_d conj(chi_q) psi_k -> sum_d du_d FFT(.)
+    static constexpr bool ZREG = true;
+    static constexpr bool REGACC = true;
+    __device__ bool regacc_grid(int) const { return true; }
+    const V *Rpsi, *Rocc, *Rchi;  // [nt][N], [ns][N], [ns][N]
+    const V *dnu;                 // [3][N] of the targets' spin
+    double2 *acc;                 // [nt][N]
+    const double *fill;
+    double b3;
+    __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
+    {
+        const size_t N = this->g.N;
+        const int tj = item / this->ns, si = item % this->ns;
+        const V rhs = cmul(__ldg(&dnu[(size_t)f * N + p]), __ldg(&Rpsi[(size_t)tj * N + p]));   // dnu_phi (:236)
+        return cmulc(__ldg(&Rchi[(size_t)si * N + p]), rhs);
+    }
+    __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
+    {
+        using S = decltype(in[0].x);
+        if constexpr (OpBase<T>::FT) {
+            const float4 c = this->fco(item, this->pidx(x, y, z), 0);
+            V r = cscale(in[0], c.y);
+            r = cadd(r, cscale(in[1], c.z));
+            return cadd(r, cscale(in[2], c.w));
+        }
+        double G[3];
+        gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
+        const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
+        const double u = this->tab_of(item)[2 * p + 1] * this->invN;
+        V r = cscale(in[0], (S)(G[0] * u));       // [3b3] sum_d du_d FFT(dnu_phi_d conj chi) (:286-295)
+        r = cadd(r, cscale(in[1], (S)(G[1] * u)));
+        return cadd(r, cscale(in[2], (S)(G[2] * u)));
+    }
+    __device__ V xyi_term(int, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        return cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p])), (decltype(v[0].x))(fill[si] * b3));
+    }
+    __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
+    __device__ void xyi_accum(int tj, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        acc_red(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p]))),
+                fill[si] * b3);
     }
 };
 
