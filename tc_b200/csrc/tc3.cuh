@@ -895,12 +895,20 @@ static int tc3_stage_ab(tcg_ctx *c, const Targets &Tg, const TRange &TR, const S
     return TCG_OK;
 }
 
+// factor of the 3a4 band part of tc3a2a4b2b5 (tc3a2a4b2b5.cpp:34-48); 3b5's is its negative
+static double band_fa4(const Host &h)
+{
+    const double Nk = h.num_kpoints, Om = h.omega;
+    const double base = 1.0 / (Nk * Nk * Om * Om);
+    return h.nspin == 1 ? base / 4.0 : base;
+}
+
 // tc2x together with stages A and B of tc3a3b3b4b6 for spin s with equal
 // Jastrow channels (OpTC2X3 + OpTC3B3 + OpTC3B): tc2x's sum goes to acc2 (the
 // H2 accumulator), 3a3 / 3b4's to qsum, 3b3 and 3b6 to acc (H3)
 template <typename T>
 static int tc2x_tc3_stage_ab(tcg_ctx *c, const TRange &TR, const Sources &S, int s, double b3, double b6,
-                             double2 *acc2, double2 *acc, double2 *qsum)
+                             double2 *acc2, double2 *acc, double2 *qsum, bool band)
 {
     using V = typename C2<T>::t;
     using OX = OpTC2X3<T>;
@@ -930,6 +938,10 @@ static int tc2x_tc3_stage_ab(tcg_ctx *c, const TRange &TR, const Sources &S, int
         x.densT = c->densT.as<V>() + 2 * N;
         x.qsum = qsum + (size_t)(TR.t0 + p.t0) * 3 * N;
         x.tmp2 = c->tmp2.as<V>();
+        x.band = band ? 1 : 0;
+        x.Qt = c->Qt.as<V>() + (S.base + p.s0) * 3 * N;
+        x.acc3 = acc + (size_t)(TR.t0 + p.t0) * N;
+        x.fa4 = band_fa4(h);
         TRY((run_chunk<T, OX>(c, x, (int)items, p.nt)));
         OY y;
         op_common<T>(c, y, p, nsl, 2);
@@ -974,7 +986,8 @@ static bool fuse_tc2x_tc3(const tcg_ctx *c, uint32_t mask)
 }
 
 template <typename T>
-static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, double2 *acc, double2 *acc2_fused)
+static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, double2 *acc, double2 *acc2_fused,
+                           bool band_fused)
 {
     PhaseScope ps_(c, "ap:tc3");
     using V = typename C2<T>::t;
@@ -996,7 +1009,7 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
         const V *dnuT = c->dnuT.as<V>() + (size_t)s * 3 * N;
         // stages A + B (with tc2x when acc2_fused is given)
         const bool eq = eq_channels(h, s);
-        if (acc2_fused) TRY((tc2x_tc3_stage_ab<T>(c, TR, S, s, b3, b6, acc2_fused, acc, qsum)));
+        if (acc2_fused) TRY((tc2x_tc3_stage_ab<T>(c, TR, S, s, b3, b6, acc2_fused, acc, qsum, band_fused)));
         else if (eq) TRY((tc3_stage_ab<T, true>(c, Tg, TR, S, s, b3, b6, acc, qsum)));
         else TRY((tc3_stage_ab<T, false>(c, Tg, TR, S, s, b3, b6, acc, qsum)));
         // 3a3: acc += a3 sum_d qsum_d dnu_d  (:629-641)
@@ -1361,17 +1374,14 @@ static int qp_stage(tcg_ctx *c)
 
 
 template <typename T>
-static int run_tc3a2a4b2b5_band(tcg_ctx *c, const Targets &Tg, double2 *acc)
+static int run_tc3a2a4b2b5_band(tcg_ctx *c, const Targets &Tg, double2 *acc, bool b5_only)
 {
     PhaseScope ps_(c, "ap:band");
     using V = typename C2<T>::t;
     const Host &h = c->h;
     const size_t N = h.N;
     const bool bitc = h.method == TCG_METHOD_BITC;
-    const double Nk = h.num_kpoints, Om = h.omega;
-    const double base = 1.0 / (Nk * Nk * Om * Om);
-    double fa4 = base, fb5 = -base;
-    if (h.nspin == 1) { fa4 /= 4.0; fb5 /= 4.0; }
+    const double fa4 = band_fa4(h), fb5 = -fa4;
     for (int s = 0; s < h.nspin; s++) {
         TRange TR = targets_of(c, Tg, s);
         Sources S = sources_of(c, s);
@@ -1381,6 +1391,18 @@ static int run_tc3a2a4b2b5_band(tcg_ctx *c, const Targets &Tg, double2 *acc)
         for (const ChunkPlan &p : plan) {
             TRY(c->tmp.ensure((size_t)p.nt * p.ns * 4 * N * sizeof(V)));
             TRY(gen_tables<T>(c, p, TAB_U_SS, s));
+            if (b5_only) {    // the 3a4 part ran in OpTC2X3
+                OpBandB<T> op;
+                op_common<T>(c, op, p, 4, 1);
+                op.Rpsi = c->Rpsi.as<V>() + (size_t)(TR.t0 + p.t0) * N;
+                op.Rocc = c->Rocc.as<V>() + (S.base + p.s0) * N;
+                op.Bt = c->Bt.as<V>() + (S.base + p.s0) * 3 * N;
+                op.acc = acc + (size_t)(TR.t0 + p.t0) * N;
+                op.fill = c->occfill.as<double>() + S.base + p.s0;
+                op.fb5 = fb5;
+                TRY((run_chunk<T, OpBandB<T>>(c, op, p.nt * p.ns, p.nt)));
+                continue;
+            }
             OpBand<T> op;
             op_common<T>(c, op, p, 4, 1);
             op.Rpsi = c->Rpsi.as<V>() + (size_t)(TR.t0 + p.t0) * N;
@@ -1684,9 +1706,11 @@ static int apply_impl(tcg_ctx *c, const ApplyArgs &A)
                            (const V *)(c->Rpsi.as<V>() + (size_t)TR.t0 * N), (const double2 *)(c->Vloc.as<double2>() + (size_t)s * N),
                            acc + (size_t)TR.t0 * N));
             }
-        if (m3 & TCG_TERM_TC3A2A4B2B5) TRY(run_tc3a2a4b2b5_band<T>(c, Tg, acc));
+        // with tc2x fused into tc3a3b3b4b6, the 3a4 band part of tc3a2a4b2b5 joins them
+        const bool band_fused = fused && (m3 & TCG_TERM_TC3A2A4B2B5);
+        if (m3 & TCG_TERM_TC3A2A4B2B5) TRY(run_tc3a2a4b2b5_band<T>(c, Tg, acc, band_fused));
         if (m3 & TCG_TERM_TC3A3B3B4B6)
-            TRY(run_tc3a3b3b4b6<T>(c, Tg, A, acc, fused ? c->acc2.as<double2>() : nullptr));
+            TRY(run_tc3a3b3b4b6<T>(c, Tg, A, acc, fused ? c->acc2.as<double2>() : nullptr, band_fused));
         TRY(finalize_acc(c, Tg, acc, A.h3, 1.0));
     }
     if (fused) {

@@ -789,6 +789,12 @@ struct OpTC2X3 : OpTC2X<T> {
     const V *densT;               // [N] n_0 + n_1 (compute precision)
     double2 *qsum;                // [nt][3][N]
     V *tmp2;                      // [items][3][N] re-forwarded grids
+    // band part of tc3a2a4b2b5 (band != 0): its outputs 0-2 are f a4 w_d too
+    // (tc3a2a4b2b5.cpp:867-875), summed times the rotated intermediate Qt_d
+    const V *Qt;                  // [ns][3][N]
+    double2 *acc3;                // [nt][N] H3 accumulator
+    double fa4;
+    int band;
     __device__ bool refwd_want(int b) const { return b > 0; }
     __device__ V refwd_load(int, int item, int, size_t p, V v) const
     {
@@ -804,6 +810,9 @@ struct OpTC2X3 : OpTC2X<T> {
         const int si = item % this->ns;
         acc_red(qsum + ((size_t)tj * 3 + (b - 1)) * N + p, to64(cmul(v[0], __ldg(&this->Rocc[(size_t)si * N + p]))),
                 this->fill[si]);
+        if (band)
+            acc_red(acc3 + (size_t)tj * N + p, to64(cmul(__ldg(&Qt[((size_t)si * 3 + (b - 1)) * N + p]), v[0])),
+                    this->fill[si] * fa4);
     }
     __device__ void xyi_accum(int tj, int item, int b, size_t p, const V *v) const
     {
@@ -948,6 +957,58 @@ struct OpBand : OpBase<T> {
         double2 *a = acc + (size_t)tj * N + p;
         if (b < 3) acc_red(a, to64(cmul(__ldg(&Qt[((size_t)si * 3 + b) * N + p]), v[0])), 1.0);    // (:875)
         else acc_red(a, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * N + p]))), fb5 * fill[si]);      // (:894)
+    }
+};
+
+// the 3b5 part of OpBand alone (its output 3), for when the 3a4 part runs in
+// OpTC2X3: inputs Bt_d psi_k, output sum_d FFT(.) du_d -> x phi_q2 (:882-894)
+template <typename T>
+struct OpBandB : OpBase<T> {
+    using V = typename C2<T>::t;
+    static constexpr const char *NAME = "bandB";
+    static constexpr int NF = 3, NB = 1;
+    static constexpr bool ZREG = true;
+    static constexpr bool REGACC = true;
+    __device__ bool regacc_grid(int) const { return true; }
+    const V *Rpsi, *Rocc;         // [nt][N], [ns][N]
+    const V *Bt;                  // [ns][3][N]
+    double2 *acc;
+    const double *fill;
+    double fb5;
+    __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
+    {
+        const size_t N = this->g.N;
+        const int tj = item / this->ns, si = item % this->ns;
+        return cmul(__ldg(&Bt[((size_t)si * 3 + f) * N + p]), __ldg(&Rpsi[(size_t)tj * N + p]));   // (:885)
+    }
+    __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
+    {
+        using S = decltype(in[0].x);
+        if constexpr (OpBase<T>::FT) {
+            const float4 c = this->fco(item, this->pidx(x, y, z), 0);
+            V r = cscale(in[0], c.x);
+            r = cadd(r, cscale(in[1], c.y));
+            return cadd(r, cscale(in[2], c.z));
+        }
+        double G[3];
+        gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
+        const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
+        const double u = this->tab_of(item)[p] * this->invN;
+        V r = cscale(in[0], (S)(G[0] * u));     // sum_d FFT(Bt_d phi_j) du0_d (:882-890)
+        r = cadd(r, cscale(in[1], (S)(G[1] * u)));
+        return cadd(r, cscale(in[2], (S)(G[2] * u)));
+    }
+    __device__ V xyi_term(int, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        return cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p])), (decltype(v[0].x))(fb5 * fill[si]));
+    }
+    __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
+    __device__ void xyi_accum(int tj, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        acc_red(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p]))),
+                fb5 * fill[si]);
     }
 };
 

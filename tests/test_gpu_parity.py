@@ -359,3 +359,21 @@ def test_36_shared_memory_accumulation(monkeypatch, method, sacc):
             ctx.set_state()
             _, g3 = ctx.apply(mask)
         assert rel(g3, r3) < MIXED_TOL
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+@pytest.mark.parametrize("method", ["TC", "BITC"])
+@pytest.mark.parametrize("fuse", [True, False])
+def test_36_shared_transforms(monkeypatch, method, fuse, prec, tol):
+    """36^3, all TC terms at once: tc2x, tc3a3b3b4b6 and the band part of
+    tc3a2a4b2b5 sharing their pair-density transforms (default) and as
+    separate passes (TCG_NO_FUSE), vs the oracle"""
+    if not fuse:
+        monkeypatch.setenv("TCG_NO_FUSE", "1")
+    s = system(method, nr=(36, 36, 36), nk=2, ecut=6.0, nbands=2, nocc=1)
+    r2, r3 = oracle_terms(s, abi.TERMS_TC)
+    with Context(s, prec) as ctx:
+        ctx.set_state()
+        g2, g3 = ctx.apply(abi.TERMS_TC)
+    assert rel(g2, r2) < tol
+    assert rel(g3, r3) < tol
