@@ -132,7 +132,7 @@ struct tcg_ctx {
     bool prune_ok = false;                  // table built and usable
     std::vector<int> prune_nact;            // host copy of the table's active-pencil counts
     bool no_prune = false;                  // TCG_NO_PRUNE: full transforms everywhere
-    bool use_sacc = false;                  // TCG_SACC: shared-memory accumulation in the 3a3b6A inverse XY pass
+    bool use_sacc = false;                  // TCG_SACC: shared-memory accumulation in the 3a3b6A and fused (2x3A) inverse XY passes
     bool no_fuse = false;                   // TCG_NO_FUSE: tc2x and tc3a3b3b4b6 run as separate passes
     bool qp_sacc = true;                    // TCG_NO_QP_SACC clears: shared-memory accumulation in the
                                             // occupied-pair inverse XY pass (36^3, FP32)

@@ -749,7 +749,7 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
     const bool sa_on = SA > 0 && op.sacc_on;
     const int nsa = sa_on ? op.sacc_n : 0;                // planes in use
     static_assert(!(Op::REFWD && Op::GS > 1), "re-forward needs GS == 1");
-    static_assert(!(SA > 0 && RACC), "shared-memory accumulation replaces the register form");
+    static_assert(!(SA > 0 && RACC && !Op::RACC_EXTRA), "shared-memory accumulation replaces the register form");
     static_assert(!(SA > 0 && Op::GS > 1 && !Op::SACC_GROUP), "grouped outputs need the op's xyi_sgroup");
     V racc[R], keep[Op::GS][R];
 #pragma unroll
@@ -805,8 +805,19 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
             continue;
         }
         const int item = op.item_of(tj, si);
+        const bool rg = RACC && op.regacc_grid(b0);
+        if (rg) {
+#pragma unroll
+            for (int k2 = 0; k2 < R; k2++) {
+                V vals[1] = {v[k2]};
+                racc[k2] = cadd(racc[k2], op.xyi_term(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals));
+                if constexpr (Op::RACC_EXTRA)
+                    if (!sa_on) op.xyi_extra(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals);
+            }
+        }
         if (sa_on) {
-            // this thread owns the accumulator points (x = l, y = t + 6 k2) of every slot
+            // this thread owns the accumulator points (x = l, y = t + 6 k2) of every slot;
+            // with the register form the slots hold the op's other accumulators
 #pragma unroll
             for (int k2 = 0; k2 < R; k2++) {
                 V vals[Op::GS];
@@ -818,13 +829,7 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
                     *a = cadd(*a, x);
                 });
             }
-        } else if (RACC && op.regacc_grid(b0)) {
-#pragma unroll
-            for (int k2 = 0; k2 < R; k2++) {
-                V vals[1] = {v[k2]};
-                racc[k2] = cadd(racc[k2], op.xyi_term(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals));
-                if constexpr (Op::RACC_EXTRA) op.xyi_extra(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals);
-            }
+        } else if (rg) {
         } else {
 #pragma unroll
             for (int k2 = 0; k2 < R; k2++) {

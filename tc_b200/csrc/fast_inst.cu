@@ -30,8 +30,7 @@ template <typename T> using OpTC3BEq = OpTC3B<T, true>;
     TCG_INST(T, OpTC3AEq<T>)           \
     TCG_INST(T, OpTC3BEq<T>)           \
     TCG_INST(T, OpTC2X3<T>)            \
-    TCG_INST(T, OpTC3B3<T>)            \
-    TCG_INST(T, OpBandB<T>)
+    TCG_INST(T, OpTC3X<T>)
 TCG_INST_ALL(float)
 TCG_INST_ALL(double)
 } // namespace tcg

@@ -904,15 +904,15 @@ static double band_fa4(const Host &h)
 }
 
 // tc2x together with stages A and B of tc3a3b3b4b6 for spin s with equal
-// Jastrow channels (OpTC2X3 + OpTC3B3 + OpTC3B): tc2x's sum goes to acc2 (the
-// H2 accumulator), 3a3 / 3b4's to qsum, 3b3 and 3b6 to acc (H3)
+// Jastrow channels (OpTC2X3 + OpTC3B): tc2x's sum goes to acc2 (the H2
+// accumulator), 3a3 / 3b4's to qsum, 3b6 (and, with band, 3a4) to acc (H3);
+// 3b3 runs later in OpTC3X
 template <typename T>
 static int tc2x_tc3_stage_ab(tcg_ctx *c, const TRange &TR, const Sources &S, int s, double b3, double b6,
                              double2 *acc2, double2 *acc, double2 *qsum, bool band)
 {
     using V = typename C2<T>::t;
     using OX = OpTC2X3<T>;
-    using OY = OpTC3B3<T>;
     using OB = OpTC3B<T, true>;
     const Host &h = c->h;
     const size_t N = h.N;
@@ -942,23 +942,15 @@ static int tc2x_tc3_stage_ab(tcg_ctx *c, const TRange &TR, const Sources &S, int
         x.Qt = c->Qt.as<V>() + (S.base + p.s0) * 3 * N;
         x.acc3 = acc + (size_t)(TR.t0 + p.t0) * N;
         x.fa4 = band_fa4(h);
+        x.sacc_on = c->use_sacc ? 1 : 0;
+        x.sacc_n = band ? 4 : 3;
         TRY((run_chunk<T, OX>(c, x, (int)items, p.nt)));
-        OY y;
-        op_common<T>(c, y, p, nsl, 2);
-        y.Rpsi = x.Rpsi;
-        y.Rocc = x.Rocc;
-        y.Rchi = x.Rchi;
-        y.dnu = c->dnuT.as<V>() + (size_t)s * 3 * N;
-        y.acc = acc + (size_t)(TR.t0 + p.t0) * N;
-        y.fill = x.fill;
-        y.b3 = b3;
-        TRY((run_chunk<T, OY>(c, y, (int)items, p.nt)));
         // 3b6B reads du from 3a3b6A's table layout (TAB_U_SX, one record for equal channels)
         TRY(gen_tables<T>(c, p, TAB_U_SX, s, 1));
         OB b;
         op_common<T>(c, b, p, nsl, 2);
         b.Rocc = x.Rocc;
-        b.acc = y.acc;
+        b.acc = acc + (size_t)(TR.t0 + p.t0) * N;
         b.tmp2 = x.tmp2;
         b.b6 = b6;
         b.s = s;
@@ -1043,7 +1035,8 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
             TRY(launch(c, k_div3b6<T>, dim3((unsigned)di.size()), dim3(256), 0, (const Div3b6Item *)c->items.p, (int)N));
             TCG_CUDA(cudaStreamSynchronize(c->stream));
         }
-        // stage C: 3b4 (:651-770)
+        // stage C: 3b4 (:651-770); after the fused first stage also 3b3 and,
+        // with band_fused, tc3a2a4b2b5's 3b5 (OpTC3X)
         std::vector<ChunkPlan> plan;
         TRY(plan_chunks(c, c->meta, TR.n, TR.key, TR.cartk, (int)S.key.size(), S.key, S.cartq,
                         max_items_for(c, 3, sizeof(V)), min_targets(c), plan));
@@ -1051,6 +1044,23 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
             const size_t items = (size_t)p.nt * p.ns;
             TRY(c->tmp.ensure(items * 3 * N * sizeof(V)));
             TRY(gen_tables<T>(c, p, TAB_U_SS, s));
+            if (acc2_fused) {
+                OpTC3X<T> op;
+                op_common<T>(c, op, p, 3, 1);
+                op.Rpsi = c->Rpsi.as<V>() + (size_t)(TR.t0 + p.t0) * N;
+                op.Rocc = c->Rocc.as<V>() + (S.base + p.s0) * N;
+                op.Rchi = (bitc ? c->Rchi.as<V>() : c->Rocc.as<V>()) + (S.base + p.s0) * N;
+                op.dnu = dnuT;
+                op.qsum = qsum + (size_t)(TR.t0 + p.t0) * 3 * N;
+                op.Bt = band_fused ? c->Bt.as<V>() + (S.base + p.s0) * 3 * N : nullptr;
+                op.acc = acc + (size_t)(TR.t0 + p.t0) * N;
+                op.fill = c->occfill.as<double>() + S.base + p.s0;
+                op.b3 = b3;
+                op.b4 = b4;
+                op.b5 = -band_fa4(h);
+                TRY((run_chunk<T, OpTC3X<T>>(c, op, (int)items, p.nt)));
+                continue;
+            }
             OpTC3C<T> op;
             op_common<T>(c, op, p, 3, 1);
             op.Rocc = c->Rocc.as<V>() + (S.base + p.s0) * N;
@@ -1374,7 +1384,7 @@ static int qp_stage(tcg_ctx *c)
 
 
 template <typename T>
-static int run_tc3a2a4b2b5_band(tcg_ctx *c, const Targets &Tg, double2 *acc, bool b5_only)
+static int run_tc3a2a4b2b5_band(tcg_ctx *c, const Targets &Tg, double2 *acc)
 {
     PhaseScope ps_(c, "ap:band");
     using V = typename C2<T>::t;
@@ -1391,18 +1401,6 @@ static int run_tc3a2a4b2b5_band(tcg_ctx *c, const Targets &Tg, double2 *acc, boo
         for (const ChunkPlan &p : plan) {
             TRY(c->tmp.ensure((size_t)p.nt * p.ns * 4 * N * sizeof(V)));
             TRY(gen_tables<T>(c, p, TAB_U_SS, s));
-            if (b5_only) {    // the 3a4 part ran in OpTC2X3
-                OpBandB<T> op;
-                op_common<T>(c, op, p, 4, 1);
-                op.Rpsi = c->Rpsi.as<V>() + (size_t)(TR.t0 + p.t0) * N;
-                op.Rocc = c->Rocc.as<V>() + (S.base + p.s0) * N;
-                op.Bt = c->Bt.as<V>() + (S.base + p.s0) * 3 * N;
-                op.acc = acc + (size_t)(TR.t0 + p.t0) * N;
-                op.fill = c->occfill.as<double>() + S.base + p.s0;
-                op.fb5 = fb5;
-                TRY((run_chunk<T, OpBandB<T>>(c, op, p.nt * p.ns, p.nt)));
-                continue;
-            }
             OpBand<T> op;
             op_common<T>(c, op, p, 4, 1);
             op.Rpsi = c->Rpsi.as<V>() + (size_t)(TR.t0 + p.t0) * N;
@@ -1708,7 +1706,7 @@ static int apply_impl(tcg_ctx *c, const ApplyArgs &A)
             }
         // with tc2x fused into tc3a3b3b4b6, the 3a4 band part of tc3a2a4b2b5 joins them
         const bool band_fused = fused && (m3 & TCG_TERM_TC3A2A4B2B5);
-        if (m3 & TCG_TERM_TC3A2A4B2B5) TRY(run_tc3a2a4b2b5_band<T>(c, Tg, acc, band_fused));
+        if ((m3 & TCG_TERM_TC3A2A4B2B5) && !band_fused) TRY(run_tc3a2a4b2b5_band<T>(c, Tg, acc));
         if (m3 & TCG_TERM_TC3A3B3B4B6)
             TRY(run_tc3a3b3b4b6<T>(c, Tg, A, acc, fused ? c->acc2.as<double2>() : nullptr, band_fused));
         TRY(finalize_acc(c, Tg, acc, A.h3, 1.0));

@@ -660,6 +660,70 @@ struct OpTC3C : OpBase<T> {
     }
 };
 
+// 3b3 (tc3a3b3b4b6.cpp:284-302), 3b4 (:651-770) and 3b5 (tc3a2a4b2b5.cpp:
+// 882-894) each transform three grids, contract them with du_d(G) =
+// (k - q + G)_d u(G; s, s) and multiply the inverse transform by phi_q f_q:
+// by linearity one transform of the sum of their scaled inputs,
+//   in_d = conj(chi_q) (b3 dnu_d psi_k + b4 qsum_d[k]) + b5 Bt_d[q] psi_k,
+// gives all three (b5 = 0 without tc3a2a4b2b5).  Runs in the second q loop,
+// after the first has completed qsum.
+template <typename T>
+struct OpTC3X : OpBase<T> {
+    using V = typename C2<T>::t;
+    static constexpr const char *NAME = "3bX";
+    static constexpr int NF = 3, NB = 1;
+    static constexpr bool ZREG = true;
+    static constexpr bool REGACC = true;
+    __device__ bool regacc_grid(int) const { return true; }
+    const V *Rpsi, *Rocc, *Rchi;  // [nt][N], [ns][N], [ns][N]
+    const V *dnu;                 // [3][N] of the targets' spin
+    const double2 *qsum;          // [nt][3][N]
+    const V *Bt;                  // [ns][3][N] or null (b5 = 0)
+    double2 *acc;
+    const double *fill;
+    double b3, b4, b5;
+    __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
+    {
+        using S = decltype(V{}.x);
+        const size_t N = this->g.N;
+        const int tj = item / this->ns, si = item % this->ns;
+        const V psi = __ldg(&Rpsi[(size_t)tj * N + p]);
+        V w = cscale(cmul(__ldg(&dnu[(size_t)f * N + p]), psi), (S)b3);
+        w = cadd(w, cscale(from64<V>(__ldg(&qsum[((size_t)tj * 3 + f) * N + p])), (S)b4));
+        V r = cmulc(__ldg(&Rchi[(size_t)si * N + p]), w);
+        if (Bt) r = cadd(r, cscale(cmul(__ldg(&Bt[((size_t)si * 3 + f) * N + p]), psi), (S)b5));
+        return r;
+    }
+    __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
+    {
+        using S = decltype(in[0].x);
+        if constexpr (OpBase<T>::FT) {
+            const float4 c = this->fco(item, this->pidx(x, y, z), 0);
+            V r = cscale(in[0], c.x);
+            r = cadd(r, cscale(in[1], c.y));
+            return cadd(r, cscale(in[2], c.z));
+        }
+        double G[3];
+        gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
+        const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
+        const double u = this->tab_of(item)[p] * this->invN;
+        V r = cscale(in[0], (S)(G[0] * u));
+        r = cadd(r, cscale(in[1], (S)(G[1] * u)));
+        return cadd(r, cscale(in[2], (S)(G[2] * u)));
+    }
+    __device__ V xyi_term(int, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        return cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p])), (decltype(v[0].x))fill[si]);
+    }
+    __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
+    __device__ void xyi_accum(int tj, int item, int, size_t p, const V *v) const
+    {
+        const int si = item % this->ns;
+        acc_red(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p]))), fill[si]);
+    }
+};
+
 // ======================================================= tc3a2a4b2b5 ops ==
 // occupied-pair stage (tc3a2a4b2b5.cpp:210-443): targets (q2, i2), sources (q1, i1).
 // EQ: u(G; sq, 0) == u(G; sq, 1), so both branches x2 = 0, 1 give the same
@@ -776,10 +840,11 @@ struct OpQP : OpBase<T> {
 // w_d = IFFT[rho G_d u(G; s, s)] are tc2x's 2b_x1 grids (tc2x.cpp:353-369) and,
 // times the filling, 3a3b6A's outputs 1-3 (tc3a3b3b4b6.cpp:305-349).  OpTC2X3
 // is tc2x with those three outputs also summed into qsum_d (3a3 / 3b4) and
-// re-forwarded times the density (3b6, for OpTC3B); OpTC3B3 is the remaining
-// 3b3 part of 3a3b6A (output 0 from the dnu inputs).  Per pair this is 12
-// transforms instead of 16.  Both read tc2x's coefficient tables (TAB_TC2X:
-// V_2body / N and G_d u(s, s) / N), which equal 3a3b6A's for equal channels.
+// re-forwarded times the density (3b6, for OpTC3B), and with band != 0 also
+// the 3a4 band part of tc3a2a4b2b5.  It reads tc2x's coefficient tables
+// (TAB_TC2X: V_2body / N and G_d u(s, s) / N), which equal 3a3b6A's for equal
+// channels.  The remaining parts that end in sum_d du_d(G) FFT[.] times phi_q
+// (3b3, 3b4, 3b5) run as one transform in OpTC3X.
 template <typename T>
 struct OpTC2X3 : OpTC2X<T> {
     using V = typename C2<T>::t;
@@ -819,56 +884,25 @@ struct OpTC2X3 : OpTC2X<T> {
         OpTC2X<T>::xyi_accum(tj, item, b, p, v);
         xyi_extra(tj, item, b, p, v);
     }
-};
-
-template <typename T>
-struct OpTC3B3 : OpBase<T> {
-    using V = typename C2<T>::t;
-    static constexpr const char *NAME = "3b3A";
-    static constexpr int NF = 3, NB = 1;     // dnu_d conj(chi_q) psi_k -> sum_d du_d FFT(.)
-    static constexpr bool ZREG = true;
-    static constexpr bool REGACC = true;
-    __device__ bool regacc_grid(int) const { return true; }
-    const V *Rpsi, *Rocc, *Rchi;  // [nt][N], [ns][N], [ns][N]
-    const V *dnu;                 // [3][N] of the targets' spin
-    double2 *acc;                 // [nt][N]
-    const double *fill;
-    double b3;
-    __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
+    // optional shared-memory accumulation of the extra sums (k_xyi_t6, FP32;
+    // tc2x's own sum stays in registers): slots 0-2 qsum_d, 3 the band part
+    static constexpr int SACC = 4;
+    static constexpr bool SACC_GROUP = true;
+    template <class F>
+    __device__ void xyi_sgroup(int, int item, int b, size_t p, const V *v, F &&add) const
+    {
+        if (b == 0) return;
+        const int si = item % this->ns;
+        using S = decltype(v[0].x);
+        const S f = (S)this->fill[si];
+        add(b - 1, cscale(cmul(v[0], __ldg(&this->Rocc[(size_t)si * this->g.N + p])), f));
+        if (band) add(3, cscale(cmul(__ldg(&Qt[((size_t)si * 3 + (b - 1)) * this->g.N + p]), v[0]), (S)(f * fa4)));
+    }
+    __device__ void xyi_sflush(int tj, int slot, size_t p, V sum) const
     {
         const size_t N = this->g.N;
-        const int tj = item / this->ns, si = item % this->ns;
-        const V rhs = cmul(__ldg(&dnu[(size_t)f * N + p]), __ldg(&Rpsi[(size_t)tj * N + p]));   // dnu_phi (:236)
-        return cmulc(__ldg(&Rchi[(size_t)si * N + p]), rhs);
-    }
-    __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
-    {
-        using S = decltype(in[0].x);
-        if constexpr (OpBase<T>::FT) {
-            const float4 c = this->fco(item, this->pidx(x, y, z), 0);
-            V r = cscale(in[0], c.y);
-            r = cadd(r, cscale(in[1], c.z));
-            return cadd(r, cscale(in[2], c.w));
-        }
-        double G[3];
-        gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
-        const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
-        const double u = this->tab_of(item)[2 * p + 1] * this->invN;
-        V r = cscale(in[0], (S)(G[0] * u));       // [3b3] sum_d du_d FFT(dnu_phi_d conj chi) (:286-295)
-        r = cadd(r, cscale(in[1], (S)(G[1] * u)));
-        return cadd(r, cscale(in[2], (S)(G[2] * u)));
-    }
-    __device__ V xyi_term(int, int item, int, size_t p, const V *v) const
-    {
-        const int si = item % this->ns;
-        return cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p])), (decltype(v[0].x))(fill[si] * b3));
-    }
-    __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
-    __device__ void xyi_accum(int tj, int item, int, size_t p, const V *v) const
-    {
-        const int si = item % this->ns;
-        acc_red(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p]))),
-                fill[si] * b3);
+        if (slot < 3) acc_red(qsum + ((size_t)tj * 3 + slot) * N + p, to64(sum), 1.0);
+        else acc_red(acc3 + (size_t)tj * N + p, to64(sum), 1.0);
     }
 };
 
@@ -957,58 +991,6 @@ struct OpBand : OpBase<T> {
         double2 *a = acc + (size_t)tj * N + p;
         if (b < 3) acc_red(a, to64(cmul(__ldg(&Qt[((size_t)si * 3 + b) * N + p]), v[0])), 1.0);    // (:875)
         else acc_red(a, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * N + p]))), fb5 * fill[si]);      // (:894)
-    }
-};
-
-// the 3b5 part of OpBand alone (its output 3), for when the 3a4 part runs in
-// OpTC2X3: inputs Bt_d psi_k, output sum_d FFT(.) du_d -> x phi_q2 (:882-894)
-template <typename T>
-struct OpBandB : OpBase<T> {
-    using V = typename C2<T>::t;
-    static constexpr const char *NAME = "bandB";
-    static constexpr int NF = 3, NB = 1;
-    static constexpr bool ZREG = true;
-    static constexpr bool REGACC = true;
-    __device__ bool regacc_grid(int) const { return true; }
-    const V *Rpsi, *Rocc;         // [nt][N], [ns][N]
-    const V *Bt;                  // [ns][3][N]
-    double2 *acc;
-    const double *fill;
-    double fb5;
-    __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
-    {
-        const size_t N = this->g.N;
-        const int tj = item / this->ns, si = item % this->ns;
-        return cmul(__ldg(&Bt[((size_t)si * 3 + f) * N + p]), __ldg(&Rpsi[(size_t)tj * N + p]));   // (:885)
-    }
-    __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
-    {
-        using S = decltype(in[0].x);
-        if constexpr (OpBase<T>::FT) {
-            const float4 c = this->fco(item, this->pidx(x, y, z), 0);
-            V r = cscale(in[0], c.x);
-            r = cadd(r, cscale(in[1], c.y));
-            return cadd(r, cscale(in[2], c.z));
-        }
-        double G[3];
-        gvec(this->rc.R, this->g, x, y, z, this->kq_of(item), G);
-        const size_t p = (size_t)x + (size_t)this->g.n0 * (y + (size_t)this->g.n1 * z);
-        const double u = this->tab_of(item)[p] * this->invN;
-        V r = cscale(in[0], (S)(G[0] * u));     // sum_d FFT(Bt_d phi_j) du0_d (:882-890)
-        r = cadd(r, cscale(in[1], (S)(G[1] * u)));
-        return cadd(r, cscale(in[2], (S)(G[2] * u)));
-    }
-    __device__ V xyi_term(int, int item, int, size_t p, const V *v) const
-    {
-        const int si = item % this->ns;
-        return cscale(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p])), (decltype(v[0].x))(fb5 * fill[si]));
-    }
-    __device__ void xyi_flush(int tj, size_t p, V s) const { acc_red(acc + (size_t)tj * this->g.N + p, to64(s), 1.0); }
-    __device__ void xyi_accum(int tj, int item, int, size_t p, const V *v) const
-    {
-        const int si = item % this->ns;
-        acc_red(acc + (size_t)tj * this->g.N + p, to64(cmul(v[0], __ldg(&Rocc[(size_t)si * this->g.N + p]))),
-                fb5 * fill[si]);
     }
 };
 
