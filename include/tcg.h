@@ -340,6 +340,25 @@ int tcg_qp_finish(tcg_ctx *ctx);
  * counterpart (TC++ has no chunked pair pipeline). */
 int tcg_set_tuning(tcg_ctx *ctx, int64_t tmp_budget_bytes);
 
+/* Kernel forms of the pass pipelines (the choices an autotuner explores; no
+ * reference counterpart).  xy: 0 = each term's default (six threads per line
+ * at 36^3), 1 = one thread per line, 2 = a lane pair per line, 3 = six
+ * threads per line; z: 0 = default, 1 = one thread per z-line, 2 = a lane
+ * pair, 3 = six threads with the inputs in shared memory, 4 = six threads
+ * with the inputs in registers.  Forms other than 0 turn the pruning of
+ * band-limited grids off (only the default kernels honour it).  Flags, each
+ * 0 or 1: prefetch (the inverse XY pass copies the next plane set while it
+ * transforms the current one), prune (band-limited grids on the pencils
+ * their support meets), fuse (tc2x, tc3a3b3b4b6 and tc3a2a4b2b5's band part
+ * share their transforms), qp_sacc / sacc (shared-memory accumulation in the
+ * occupied-pair / first-stage inverse XY passes).  min_targets: targets per
+ * chunk (0 = default).  tcg_get_forms reads the current choice. */
+typedef struct tcg_forms {
+    int32_t xy, z, prefetch, prune, fuse, qp_sacc, sacc, min_targets;
+} tcg_forms;
+int tcg_set_forms(tcg_ctx *ctx, const tcg_forms *forms);
+int tcg_get_forms(tcg_ctx *ctx, tcg_forms *forms);
+
 /* Per-kernel timing with CUDA events recorded on the context stream around
  * every launch (off by default; enabling clears earlier records).  No
  * reference counterpart (TC++ times whole phases at 1 s resolution,

@@ -55,6 +55,8 @@ def lib():
         L.tcg_gram_schmidt.argtypes = [C.c_int32, C.c_int32, vp, vp, vp]
         L.tcg_davidson_expand.argtypes = [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp,
                                           C.POINTER(C.c_double), C.POINTER(C.c_int32), vp]
+        L.tcg_set_forms.argtypes = [vp, C.POINTER(abi.Forms)]
+        L.tcg_get_forms.argtypes = [vp, C.POINTER(abi.Forms)]
         L.tcg_energy.argtypes = [vp, C.POINTER(C.c_int32), vp, vp, C.POINTER(C.c_double)]
         _lib = L
     return _lib
@@ -69,4 +71,4 @@ EXPORTS = ["tcg_ctx_create", "tcg_ctx_destroy", "tcg_set_state", "tcg_apply", "t
            "tcg_sum_of_vaux", "tcg_density", "tcg_stream", "tcg_launch_count", "tcg_last_error",
            "tcg_version", "tcg_set_tuning", "tcg_profile", "tcg_profile_read", "tcg_refresh_state",
            "tcg_sum_of_vaux_noalloc", "tcg_energy", "tcg_qp_partial", "tcg_qp_finish", "tcg_set_pseudo", "tcg_apply_h1", "tcg_energy_grad",
-           "tcg_subspace_ritz", "tcg_gram_schmidt", "tcg_davidson_expand"]
+           "tcg_subspace_ritz", "tcg_gram_schmidt", "tcg_davidson_expand", "tcg_set_forms", "tcg_get_forms"]

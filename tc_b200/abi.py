@@ -88,6 +88,10 @@ class StateDesc(C.Structure):
     ]
 
 
+class Forms(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("xy", "z", "prefetch", "prune", "fuse", "qp_sacc", "sacc", "min_targets")]
+
+
 class PseudoDesc(C.Structure):
     _fields_ = [
         ("vloc", _f64p),

@@ -75,6 +75,22 @@ class Context:
     def set_tuning(self, tmp_budget):
         check(lib().tcg_set_tuning(self.handle, int(tmp_budget)))
 
+    def forms(self):
+        """The kernel forms in use (tcg_get_forms) as a dict."""
+        f = abi.Forms()
+        check(lib().tcg_get_forms(self.handle, C.byref(f)))
+        return {n: int(getattr(f, n)) for n, _ in abi.Forms._fields_}
+
+    def set_forms(self, **kw):
+        """Change some kernel forms (tcg_set_forms); the others keep their value."""
+        cur = self.forms()
+        unknown = set(kw) - set(cur)
+        if unknown:
+            raise KeyError(f"unknown kernel forms {sorted(unknown)}")
+        cur.update({k: int(v) for k, v in kw.items()})
+        f = abi.Forms(**cur)
+        check(lib().tcg_set_forms(self.handle, C.byref(f)))
+
     # -- state ----------------------------------------------------------------
     def set_state(self, system=None):
         s = system or self.system

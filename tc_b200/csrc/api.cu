@@ -547,6 +547,37 @@ extern "C" int tcg_set_tuning(tcg_ctx *c, int64_t tmp_budget_bytes)
     return TCG_OK;
 }
 
+extern "C" int tcg_set_forms(tcg_ctx *c, const tcg_forms *f)
+{
+    if (!c || !f) return fail(TCG_ERR_ARG, "null argument");
+    if (f->xy < 0 || f->xy > 3 || f->z < 0 || f->z > 4 || f->min_targets < 0)
+        return fail(TCG_ERR_ARG, "bad kernel form");
+    if (c->fast_n != 36 && (f->xy == 3 || f->z >= 3)) return fail(TCG_ERR_UNSUPPORTED, "six-thread forms need a 36^3 grid");
+    c->xy_kernels = f->xy;
+    c->z_kernels = f->z;
+    c->no_prefetch = !f->prefetch;
+    c->no_prune = !f->prune;
+    c->no_fuse = !f->fuse;
+    c->qp_sacc = f->qp_sacc != 0;
+    c->use_sacc = f->sacc != 0;
+    c->min_targets = f->min_targets;
+    return TCG_OK;
+}
+
+extern "C" int tcg_get_forms(tcg_ctx *c, tcg_forms *f)
+{
+    if (!c || !f) return fail(TCG_ERR_ARG, "null argument");
+    f->xy = c->xy_kernels;
+    f->z = c->z_kernels;
+    f->prefetch = c->no_prefetch ? 0 : 1;
+    f->prune = c->no_prune ? 0 : 1;
+    f->fuse = c->no_fuse ? 0 : 1;
+    f->qp_sacc = c->qp_sacc ? 1 : 0;
+    f->sacc = c->use_sacc ? 1 : 0;
+    f->min_targets = c->min_targets;
+    return TCG_OK;
+}
+
 // ------------------------------------------------------ divergence sums --
 // one block per (irreducible k, all-k q): shells until the shell sum drops
 // below 1e-20 (potentials_coulomb.cpp:118-139), fixed-tree block reduction.

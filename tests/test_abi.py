@@ -61,11 +61,14 @@ def test_struct_layout_matches_header(tmp_path):
     src = tmp_path / "size_probe.c"
     exe = tmp_path / "size_probe"
     src.write_text('#include "include/tcg.h"\n#include <stdio.h>\n'
-                   'int main(){printf("%zu %zu\\n", sizeof(tcg_system_desc), sizeof(tcg_state_desc));}\n')
+                   'int main(){printf("%zu %zu %zu %zu\\n", sizeof(tcg_system_desc), sizeof(tcg_state_desc), '
+                   'sizeof(tcg_pseudo_desc), sizeof(tcg_forms));}\n')
     subprocess.run(["gcc", "-I", ROOT, "-o", str(exe), str(src)], check=True)
-    a, b = map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split())
+    a, b, c, d = map(int, subprocess.run([str(exe)], capture_output=True, text=True).stdout.split())
     assert C.sizeof(abi.SystemDesc) == a
     assert C.sizeof(abi.StateDesc) == b
+    assert C.sizeof(abi.PseudoDesc) == c
+    assert C.sizeof(abi.Forms) == d
 
 
 def test_oracle_exports():
