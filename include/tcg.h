@@ -300,12 +300,15 @@ int tcg_sum_of_vaux(const tcg_system_desc *sys, double *alpha_out, double *sum_v
  * call then copies a convergence flag to the host and synchronises that
  * stream before it returns.  Scratch is a static device array of 16384
  * (k, q) pairs held by every GPU that loads the library until the process
- * exits; larger nk_irr * nk_all is rejected with TCG_ERR_ARG.  The first call
- * on a device looks the array's device address up (cudaGetSymbolAddress)
- * and keeps it for the life of the process: after a cudaDeviceReset of that
- * device the kept address is stale and the entry point must not be called
- * again.  Every call shares the one array: calls that overlap on the GPU
- * (other threads or streams) race and must be serialised by the caller. */
+ * exits; larger nk_irr * nk_all is rejected with TCG_ERR_ARG, as are a
+ * non-finite recip or omega.  A k-vector difference that is not finite or
+ * beyond +-64 fails with TCG_ERR_NUMERIC.  Set-up: the first call on a device
+ * looks the array's device address up (cudaGetSymbolAddress, with that device
+ * current) and keeps it for the life of the process, so make that first call
+ * before any stream capture begins; after a cudaDeviceReset of that device
+ * the kept address is stale and the entry point must not be called again.
+ * Every call shares the one array: calls that overlap on the GPU (other
+ * threads or streams) race and must be serialised by the caller. */
 int tcg_sum_of_vaux_noalloc(const double recip[9], double omega, int32_t nk_irr, int32_t nk_all,
                             const double *kirr_dev, const double *kall_dev, double *sum_vaux_dev,
                             double *alpha_out, void *stream);

@@ -587,11 +587,25 @@ __global__ void k_sum_vaux(int nk_all, const double *kirr, const double *kall, R
     const int ik = blockIdx.x / nk_all, a = blockIdx.x % nk_all;
     __shared__ double red[256];
     double kq[3];
+    bool in_range = true;
     for (int d = 0; d < 3; d++) {
         double v = kirr[3 * ik + d] - kall[3 * a + d];
+        // fractional coordinates: a difference that is not finite or beyond
+        // +-64 is no k-vector, and the wrap loops below would not end on it
+        if (!(fabs(v) < 64.0)) {
+            in_range = false;
+            v = 0.0;
+        }
         while (v < -1e-8) v += 1.0;
         while (v > 1.0 - 1e-8) v -= 1.0;
         kq[d] = v;
+    }
+    if (!in_range) {  // the same for every thread of the block
+        if (threadIdx.x == 0) {
+            partial[blockIdx.x] = 0.0;
+            match[blockIdx.x] = 2;
+        }
+        return;
     }
     const bool m = kq[0] * kq[0] + kq[1] * kq[1] + kq[2] * kq[2] < 1e-8;
     double total = 0.0;
@@ -666,7 +680,7 @@ extern "C" int tcg_sum_of_vaux(const tcg_system_desc *sys, double *alpha_out, do
         bool m = false;
         for (int a = 0; a < nk_all; a++) {
             const int f = match[(size_t)k * nk_all + a];
-            if (f & 2) return fail(TCG_ERR_NUMERIC, "divergence shell sum did not converge");
+            if (f & 2) return fail(TCG_ERR_NUMERIC, "divergence shell sum did not converge (or a k-vector difference is not finite or beyond +-64)");
             m = m || (f & 1);
             total += part[(size_t)k * nk_all + a];
         }
@@ -1018,7 +1032,9 @@ extern "C" int tcg_sum_of_vaux_noalloc(const double recip[9], double omega, int3
                                        double *alpha_out, void *stream)
 {
     if (!recip || !kirr_dev || !kall_dev || !sum_vaux_dev) return fail(TCG_ERR_ARG, "null argument");
-    if (!(omega > 0)) return fail(TCG_ERR_ARG, "unit-cell volume must be positive");
+    if (!(omega > 0) || !std::isfinite(omega)) return fail(TCG_ERR_ARG, "unit-cell volume must be positive and finite");
+    for (int i = 0; i < 9; i++)
+        if (!std::isfinite(recip[i])) return fail(TCG_ERR_ARG, "non-finite reciprocal lattice vector");
     if (nk_irr < 1 || nk_all < 1) return fail(TCG_ERR_ARG, "no k-points");
     if ((int64_t)nk_irr * nk_all > TCG_NOALLOC_MAX_PAIRS)
         return fail(TCG_ERR_ARG, "nk_irr * nk_all exceeds the 16384 (k, q) pairs of the static scratch");
@@ -1041,7 +1057,7 @@ extern "C" int tcg_sum_of_vaux_noalloc(const double recip[9], double omega, int3
     int err = 0;
     TCG_CUDA(cudaMemcpyAsync(&err, sc.err, sizeof(int), cudaMemcpyDeviceToHost, st));
     TCG_CUDA(cudaStreamSynchronize(st));
-    if (err) return fail(TCG_ERR_NUMERIC, "divergence shell sum did not converge");
+    if (err) return fail(TCG_ERR_NUMERIC, "divergence shell sum did not converge (or a k-vector difference is not finite or beyond +-64)");
     if (alpha_out) *alpha_out = alpha;
     return TCG_OK;
 }

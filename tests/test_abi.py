@@ -55,6 +55,32 @@ def test_version_and_error_without_gpu(lib):
     assert e.value.code == 2            # TCG_ERR_CUDA: no device, no fallback
 
 
+def test_noalloc_rejects_arguments_before_device_work():
+    """tcg_sum_of_vaux_noalloc checks its host arguments before it touches
+    the device: oversize k-sets, non-finite or non-positive geometry and null
+    pointers are TCG_ERR_ARG (the device pointers are never dereferenced)."""
+    from tc_b200 import TCError, synth
+    from tc_b200.context import sum_of_vaux_noalloc
+    s = synth.config("C1")
+    fake = 16  # never used: every case fails on the host
+
+    class Geo:
+        recip = s.recip
+        omega = s.omega
+        nk_irr = s.nk_irr
+        nk_all = s.nk_all
+    cases = [dict(nk_irr=129, nk_all=128), dict(omega=0.0), dict(omega=float("inf")),
+             dict(recip=np.where(np.eye(3) > 0, np.nan, np.asarray(s.recip))), dict(nk_irr=0)]
+    for kw in cases:
+        g = type("G", (Geo,), kw)
+        with pytest.raises(TCError) as e:
+            sum_of_vaux_noalloc(g, fake, fake, fake)
+        assert e.value.code == 1, kw
+    with pytest.raises(TCError) as e:
+        sum_of_vaux_noalloc(Geo, 0, fake, fake)
+    assert e.value.code == 1
+
+
 def test_struct_layout_matches_header(tmp_path):
     """ctypes mirrors of the descriptors have the C sizes (compiled check)"""
     from tc_b200 import abi

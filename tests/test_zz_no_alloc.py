@@ -60,3 +60,25 @@ def test_noalloc_rejects_oversize():
         nk_all = 200
     with pytest.raises(TCError):
         sum_of_vaux_noalloc(Big, k.data_ptr(), k.data_ptr(), out.data_ptr())
+
+
+def test_noalloc_rejects_nonfinite_k():
+    """A NaN k-vector sets the failure flag of its (k, q) blocks before the
+    fractional wrap loops; the call returns TCG_ERR_NUMERIC, and the next call
+    with good inputs is unaffected."""
+    import torch
+    from tc_b200 import TCError
+    s = synth.config("C1")
+    dev = torch.device("cuda", 0)
+    kirr = np.ascontiguousarray(s.kvec[s.kall_off[:-1]]).copy()
+    kirr[0, 1] = np.nan
+    kirr_t = torch.from_numpy(kirr).to(dev)
+    kall_t = torch.from_numpy(np.ascontiguousarray(s.kvec)).to(dev)
+    out = torch.zeros(s.nk_irr, dtype=torch.float64, device=dev)
+    with pytest.raises(TCError):
+        sum_of_vaux_noalloc(s, kirr_t.data_ptr(), kall_t.data_ptr(), out.data_ptr())
+    alpha_ref, ref = sum_of_vaux(s)
+    kirr_t.copy_(torch.from_numpy(np.ascontiguousarray(s.kvec[s.kall_off[:-1]])))
+    sum_of_vaux_noalloc(s, kirr_t.data_ptr(), kall_t.data_ptr(), out.data_ptr())
+    torch.cuda.synchronize()
+    assert np.abs(out.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
