@@ -965,13 +965,12 @@ static bool eq_channels(const Host &h, int s)
     return h.A[0 * 2 + s] == h.A[1 * 2 + s] && h.F[0 * 2 + s] == h.F[1 * 2 + s];
 }
 
-// tc2x runs fused with tc3a3b3b4b6 (tc2x_tc3_stage_ab) when both are applied,
-// at 36^3 with the default kernel forms, equal channels for every spin
+// tc2x runs fused with tc3a3b3b4b6 (tc2x_tc3_stage_ab) when both are applied
+// and every spin has equal Jastrow channels (any grid and kernel form)
 static bool fuse_tc2x_tc3(const tcg_ctx *c, uint32_t mask)
 {
     const Host &h = c->h;
     if (c->no_fuse || !(mask & TCG_TERM_TC2X) || !(mask & TCG_TERM_TC3A3B3B4B6)) return false;
-    if (c->fast_n != 36 || c->force_generic || c->xy_kernels != 0 || c->z_kernels != 0) return false;
     for (int s = 0; s < h.nspin; s++)
         if (!eq_channels(h, s)) return false;
     return true;
