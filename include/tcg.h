@@ -344,12 +344,13 @@ int tcg_qp_finish(tcg_ctx *ctx);
 int tcg_set_tuning(tcg_ctx *ctx, int64_t tmp_budget_bytes);
 
 /* Kernel forms of the pass pipelines (the choices an autotuner explores; no
- * reference counterpart).  xy: 0 = each term's default (six threads per line
- * at 36^3), 1 = one thread per line, 2 = a lane pair per line, 3 = six
- * threads per line; z: 0 = default, 1 = one thread per z-line, 2 = a lane
- * pair, 3 = six threads with the inputs in shared memory, 4 = six threads
- * with the inputs in registers.  Forms other than 0 turn the pruning of
- * band-limited grids off (only the default kernels honour it).  Flags, each
+ * reference counterpart).  xy: 0 = each term's default (split lines on the
+ * grids that have them), 1 = one thread per line, 2 = a lane pair per line,
+ * 3 = split lines (six threads per line at 36^3, four at 48^3); z: 0 =
+ * default, 1 = one thread per z-line, 2 = a lane pair, 3 = split lines with
+ * the inputs in shared memory, 4 = split lines with the inputs in registers
+ * (3 and 4 need a 36^3 or 48^3 grid).  xy 1 or 2 and z 1 or 2 turn the
+ * pruning of band-limited grids off (only the split-line kernels honour it).  Flags, each
  * 0 or 1: prefetch (the inverse XY pass copies the next plane set while it
  * transforms the current one), prune (band-limited grids on the pencils
  * their support meets), fuse (tc2x, tc3a3b3b4b6 and tc3a2a4b2b5's band part

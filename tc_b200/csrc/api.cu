@@ -300,7 +300,7 @@ extern "C" int tcg_ctx_create(const tcg_system_desc *sys, int32_t precision, tcg
     if (getenv("TCG_SACC")) c->use_sacc = true;
     if (getenv("TCG_NO_QP_SACC")) c->qp_sacc = false;
     if (getenv("TCG_NO_FUSE")) c->no_fuse = true;
-    if (c->fast_n == 36 && (rc = build_prune_table(c)) != TCG_OK) {
+    if (split_line_grid(c->fast_n) && (rc = build_prune_table(c)) != TCG_OK) {
         tcg_ctx_destroy(c);
         return rc;
     }
@@ -552,7 +552,8 @@ extern "C" int tcg_set_forms(tcg_ctx *c, const tcg_forms *f)
     if (!c || !f) return fail(TCG_ERR_ARG, "null argument");
     if (f->xy < 0 || f->xy > 3 || f->z < 0 || f->z > 4 || f->min_targets < 0)
         return fail(TCG_ERR_ARG, "bad kernel form");
-    if (c->fast_n != 36 && (f->xy == 3 || f->z >= 3)) return fail(TCG_ERR_UNSUPPORTED, "six-thread forms need a 36^3 grid");
+    if (!split_line_grid(c->fast_n) && (f->xy == 3 || f->z >= 3))
+        return fail(TCG_ERR_UNSUPPORTED, "split-line kernel forms need a 36^3 or 48^3 grid");
     c->xy_kernels = f->xy;
     c->z_kernels = f->z;
     c->no_prefetch = !f->prefetch;

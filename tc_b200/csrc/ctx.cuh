@@ -92,6 +92,11 @@ struct Host {
     std::vector<size_t> g0_off;             // [nspin*nk] offset of (s, k) in gidx0
 };
 
+// cubic grid sizes whose pass kernels split each line over several threads
+// (fast::t6::ShapeOf: 36 = 6 x 6, 48 = 4 x 12); only those forms honour
+// pruned transforms
+inline bool split_line_grid(int n) { return n == 36 || n == 48; }
+
 struct tcg_ctx_impl;
 } // namespace tcg
 
@@ -148,10 +153,11 @@ struct tcg_ctx {
     int ftab_nrec = 1;
     int fast_n = 0;                         // cubic grid size with compiled fast kernels (0: generic path)
     bool force_generic = false;             // use the generic pass kernels even if fast_n is set
-    int xy_kernels = 0;                     // fast XY passes: 0 default, 1 all line, 2 all lane-pair, 3 six threads per line (36^3)
+    int xy_kernels = 0;                     // fast XY passes: 0 default, 1 all line, 2 all lane-pair, 3 split lines (36^3, 48^3)
     bool no_prefetch = false;               // fast XYI: no prefetch of the next plane set
     const char *stage = "misc";            // profiling tag of untagged launches (the current stage)
-    int z_kernels = 0;                      // fast Z pass: 0 per-term choice, 1 one thread per line, 2 lane pairs
+    int z_kernels = 0;                      // fast Z pass: 0 per-term choice, 1 one thread per line, 2 lane pairs,
+                                            // 3 / 4 split lines in shared memory / registers (36^3, 48^3)
     size_t tmp_budget = 0;                  // bytes per chunk of pass temporaries (0: default 8 GiB)
     int min_targets = 0;                    // targets per chunk (0: default, about 12 waves of XYI CTAs)
     int64_t launches = 0;

@@ -614,75 +614,119 @@ __global__ void __launch_bounds__(Cfg<N, sizeof(typename C2<T>::t)>::THREADS, 2)
     }
 }
 
-// ------------------------------------------ XY passes, 36 = 6 x 6, t6 --
-// For N = 36 each line is transformed by six threads in two radix-6 stages
-// (Cooley-Tukey, 36 = 6 x 6) exchanged through the plane in shared memory:
-// stage 1, thread t: u_t[k1] = w36^{t k1} DFT6_m(x[t + 6 m]);
-// stage 2, thread t as k1: X[k1 + 6 k2] = DFT6_t'(u_t'[k1]).
-// A thread holds 6 values instead of 36, so a CTA of one plane (216
-// threads) needs few registers and many CTAs stay resident.  Thread mapping
-// r = t * 36 + l: consecutive lanes own consecutive lines l, so the row
-// sweeps (stride 37) and the column sweeps (stride 1 across lanes) are free
-// of bank conflicts and the global copies are coalesced along x.
+// ------------------------------- XY and Z passes, several threads per line --
+// For N = TL * M with TL | M (36 = 6 x 6, 48 = 4 x 12) each line is
+// transformed by TL threads in two stages (Cooley-Tukey, n = t + TL m,
+// k = k1 + M k2), exchanged once through the plane in shared memory:
+//   stage 1, thread t: u_t[k1] = w_N^{t k1} DFT_M over m of x[t + TL m];
+//   stage 2, thread t for k1 = t + TL c (c < M / TL):
+//            X[k1 + M k2] = DFT_TL over t' of u_t'[k1].
+// Thread t holds the line at positions t + TL m (m < M) both before and after
+// the transform: X[t + TL m'] in v[m'], m' = c + (M / TL) k2.  A thread
+// holds M values instead of N, so a CTA of one plane (TL N threads) needs
+// few registers and many CTAs stay resident.  Thread mapping r = t * N + l:
+// consecutive lanes own consecutive lines l, so the row sweeps (odd stride
+// PAD) and the column sweeps (stride 1 across lanes) are free of bank
+// conflicts and the global copies are coalesced along x.
 namespace t6 {
-constexpr int N = 36, R = 6, PAD = 37, THREADS = R * N;
+template <int N_, int TL_> struct Shape {
+    static constexpr int N = N_, TL = TL_, M = N_ / TL_;
+    static constexpr int PAD = N_ + ((N_ % 2 == 0) ? 1 : 0);
+    static constexpr int THREADS = TL_ * N_;     // XY passes: one plane per CTA
+    static constexpr int ZTHREADS = TL_ * 32;    // Z passes: 32 pencils per CTA
+    // resident CTAs per SM the launch bounds ask for (register budget)
+    static constexpr int MINB = M <= 6 ? 4 : 3;
+    static constexpr int MINB_ZR = M <= 6 ? 3 : 2;
+    static_assert(N_ % (TL_ * TL_) == 0, "two-stage lines need TL | N / TL");
+    static_assert(N_ <= 64 && M <= 32 && TL_ <= 32, "pencil masks and twiddle slots");
+};
+// threads per line of each compiled grid size (0: one-thread-per-line forms only)
+template <int N> struct ShapeOf { static constexpr int TL = 0; };
+template <> struct ShapeOf<36> { static constexpr int TL = 6; };
+template <> struct ShapeOf<48> { static constexpr int TL = 4; };
 
 template <typename V>
 struct Tw {
-    const V *w;    // [36] exp(-2 pi i j/36)
-    const V *w6;   // [6]  exp(-2 pi i j/6)
+    const V *w;    // [N]  exp(-2 pi i j/N)
+    const V *wm;   // [M]  exp(-2 pi i j/M)
+    const V *wt;   // [TL] exp(-2 pi i j/TL)
 };
 
-// line element i at base[i * stride]; all threads of the CTA call it.
-// On return v[k2] = X[t + 6 k2]; NAT: also written back in natural order.
-template <typename V, int DIR, bool NAT>
-__device__ __forceinline__ void xform(V *base, int stride, int t, const Tw<V> &tw, V (&v)[R])
+// stage 1 of thread t on u[m] = x[t + TL m]: DFT_M, then the twiddles
+template <typename V, class S, int DIR>
+__device__ __forceinline__ void stage1(V (&u)[S::M], int t, const Tw<V> &tw)
 {
-    V u[R];
+    line_fft<V, S::M, DIR>(u, tw.wm);
 #pragma unroll
-    for (int m = 0; m < R; m++) u[m] = base[(t + R * m) * stride];
-    line_fft<V, R, DIR>(u, tw.w6);
-#pragma unroll
-    for (int k1 = 1; k1 < R; k1++) {
+    for (int k1 = 1; k1 < S::M; k1++) {
         V w = tw.w[t * k1];
         if (DIR > 0) w.y = -w.y;
         u[k1] = cmul(u[k1], w);
     }
+}
+// stage 2 of thread t from the exchanged values (u_j[k1] at
+// base[(k1 TL + j) stride]): X[t + TL m'] into v[m']
+template <typename V, class S, int DIR>
+__device__ __forceinline__ void stage2(const V *base, int stride, int t, const Tw<V> &tw, V (&v)[S::M])
+{
+    constexpr int C = S::M / S::TL;
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+        const int k1 = t + S::TL * c;
+        V w[S::TL];
+#pragma unroll
+        for (int j = 0; j < S::TL; j++) w[j] = base[(k1 * S::TL + j) * stride];
+        line_fft<V, S::TL, DIR>(w, tw.wt);
+#pragma unroll
+        for (int k2 = 0; k2 < S::TL; k2++) v[c + C * k2] = w[k2];
+    }
+}
+
+// line element i at base[i * stride]; all threads of the CTA call it.
+// On return v[m] = X[t + TL m]; NAT: also written back in natural order.
+template <typename V, class S, int DIR, bool NAT>
+__device__ __forceinline__ void xform(V *base, int stride, int t, const Tw<V> &tw, V (&v)[S::M])
+{
+    V u[S::M];
+#pragma unroll
+    for (int m = 0; m < S::M; m++) u[m] = base[(t + S::TL * m) * stride];
+    stage1<V, S, DIR>(u, t, tw);
     __syncthreads();
 #pragma unroll
-    for (int k1 = 0; k1 < R; k1++) base[(k1 * R + t) * stride] = u[k1];
+    for (int k1 = 0; k1 < S::M; k1++) base[(k1 * S::TL + t) * stride] = u[k1];
     __syncthreads();
-#pragma unroll
-    for (int j = 0; j < R; j++) v[j] = base[(t * R + j) * stride];
-    line_fft<V, R, DIR>(v, tw.w6);
+    stage2<V, S, DIR>(base, stride, t, tw, v);
     if (NAT) {
         __syncthreads();
 #pragma unroll
-        for (int k2 = 0; k2 < R; k2++) base[(t + R * k2) * stride] = v[k2];
+        for (int m = 0; m < S::M; m++) base[(t + S::TL * m) * stride] = v[m];
         __syncthreads();
     }
 }
 
-template <typename V>
+// twiddle tables in shared memory: N at 0, M at 64, TL at 96 (128 slots)
+template <typename V, class S>
 __device__ __forceinline__ Tw<V> stage(const GridDesc &g, V *tws)
 {
     const V *src = twsrc<V>(g);
-    for (int i = threadIdx.x; i < N; i += blockDim.x) tws[i] = src[i];
+    for (int i = threadIdx.x; i < S::N; i += blockDim.x) tws[i] = src[i];
     __syncthreads();
-    if (threadIdx.x < R) tws[64 + threadIdx.x] = tws[R * threadIdx.x];
+    if (threadIdx.x < S::M) tws[64 + threadIdx.x] = tws[S::TL * threadIdx.x];
+    if (threadIdx.x < S::TL) tws[96 + threadIdx.x] = tws[S::M * threadIdx.x];
     __syncthreads();
-    return Tw<V>{tws, tws + 64};
+    return Tw<V>{tws, tws + 64, tws + 96};
 }
 
 // XYF: one (item, z) plane per CTA; pair products -> forward XY FFT -> tmp
-template <typename T, class Op>
-__global__ void __launch_bounds__(THREADS, 4) k_xyf_t6(Op op, int nplanes)
+template <typename T, class Op, class S>
+__global__ void __launch_bounds__(S::THREADS, S::MINB) k_xyf_t6(Op op, int nplanes)
 {
     using V = typename C2<T>::t;
+    constexpr int N = S::N, TL = S::TL, M = S::M, PAD = S::PAD;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tws = reinterpret_cast<V *>(smem_raw);
     V *A = tws + 128;                     // [N][PAD]
-    const Tw<V> tw = stage<V>(op.g, tws);
+    const Tw<V> tw = stage<V, S>(op.g, tws);
     const int t = threadIdx.x / N, l = threadIdx.x % N;
     const int pid = blockIdx.x;
     if (pid >= nplanes) return;           // uniform over the CTA
@@ -691,23 +735,23 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyf_t6(Op op, int nplanes)
     for (int f = 0; f < Op::NF; f++) {
         __syncthreads();
 #pragma unroll
-        for (int m = 0; m < R; m++) {
-            const int y = t + R * m;
+        for (int m = 0; m < M; m++) {
+            const int y = t + TL * m;
             A[y * PAD + l] = op.xyf_load(item, f, l, y, z, pz + (size_t)y * N + l);
         }
         __syncthreads();
-        V v[R];
-        xform<V, -1, true>(A + l * PAD, 1, t, tw, v);      // rows
-        xform<V, -1, false>(A + l, PAD, t, tw, v);         // columns: v[k2] at y = t + 6 k2
+        V v[M];
+        xform<V, S, -1, true>(A + l * PAD, 1, t, tw, v);      // rows
+        xform<V, S, -1, false>(A + l, PAD, t, tw, v);         // columns: v[m] at y = t + TL m
         V *dst = op.tmp_grid(item, f) + pz + l;
         if (((Op::BLI >> f) & 1) && op.m.prune) {
             const unsigned long long bits = op.pcol(item, l);
 #pragma unroll
-            for (int k2 = 0; k2 < R; k2++)
-                if ((bits >> (t + R * k2)) & 1) dst[(size_t)(t + R * k2) * N] = v[k2];
+            for (int m = 0; m < M; m++)
+                if ((bits >> (t + TL * m)) & 1) dst[(size_t)(t + TL * m) * N] = v[m];
         } else {
 #pragma unroll
-            for (int k2 = 0; k2 < R; k2++) dst[(size_t)(t + R * k2) * N] = v[k2];
+            for (int m = 0; m < M; m++) dst[(size_t)(t + TL * m) * N] = v[m];
         }
     }
 }
@@ -729,15 +773,16 @@ __device__ __forceinline__ void sacc_group(const Op &op, int tj, int item, int b
 // XYI: one (target, z) plane per CTA, looping over the chunk's (source,
 // output) steps; the next step's plane is copied asynchronously into the
 // second set.  GS > 1: the first GS - 1 outputs of a group wait in registers.
-template <typename T, class Op>
-__global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
+template <typename T, class Op, class S>
+__global__ void __launch_bounds__(S::THREADS, S::MINB) k_xyi_t6(Op op, int nplanes)
 {
     using V = typename C2<T>::t;
+    constexpr int N = S::N, TL = S::TL, M = S::M, PAD = S::PAD;
     constexpr int PS = N * PAD;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tws = reinterpret_cast<V *>(smem_raw);
     V *W = tws + 128;                     // [2][N][PAD]
-    const Tw<V> tw = stage<V>(op.g, tws);
+    const Tw<V> tw = stage<V, S>(op.g, tws);
     const int t = threadIdx.x / N, l = threadIdx.x % N;
     const int pid = blockIdx.x;
     if (pid >= nplanes) return;           // uniform over the CTA
@@ -751,10 +796,10 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
     static_assert(!(Op::REFWD && Op::GS > 1), "re-forward needs GS == 1");
     static_assert(!(SA > 0 && RACC && !Op::RACC_EXTRA), "shared-memory accumulation replaces the register form");
     static_assert(!(SA > 0 && Op::GS > 1 && !Op::SACC_GROUP), "grouped outputs need the op's xyi_sgroup");
-    V racc[R], keep[Op::GS][R];
+    V racc[M], keep[Op::GS][M];
 #pragma unroll
-    for (int i = 0; i < R; i++) racc[i] = czero<V>();
-    V *SAcc = W + 2 * PS;                 // [SA][N][N]: this thread owns y = t + 6 k2, x = l
+    for (int i = 0; i < M; i++) racc[i] = czero<V>();
+    V *SAcc = W + 2 * PS;                 // [SA][N][N]: this thread owns y = t + TL m, x = l
     // pruned chunks: the pencil-table entry of every source, looked up once
     // (the copies of each step then need one load of their column mask)
     int *sent = reinterpret_cast<int *>(SAcc + (size_t)nsa * N * N);
@@ -764,7 +809,7 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
     }
     for (int a = 0; a < nsa; a++)
 #pragma unroll
-        for (int k2 = 0; k2 < R; k2++) SAcc[(a * N + t + R * k2) * N + l] = czero<V>();
+        for (int m = 0; m < M; m++) SAcc[(a * N + t + TL * m) * N + l] = czero<V>();
     const int total = ns * Op::NB;        // it = si * NB + b
     auto issue = [&](int it) {
         const int item = op.item_of(tj, it / Op::NB), b = it % Op::NB;
@@ -774,13 +819,13 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
             // band-limited output: the Z pass wrote only the pencils its support meets
             const unsigned long long bits = op.m.pbits[(size_t)sent[it / Op::NB] * op.g.n0 + l];
 #pragma unroll
-            for (int m = 0; m < R; m++) {
-                if ((bits >> (t + R * m)) & 1) cp_async_elem(dst + (t + R * m) * PAD, src + (size_t)(t + R * m) * N);
-                else dst[(t + R * m) * PAD] = czero<V>();
+            for (int m = 0; m < M; m++) {
+                if ((bits >> (t + TL * m)) & 1) cp_async_elem(dst + (t + TL * m) * PAD, src + (size_t)(t + TL * m) * N);
+                else dst[(t + TL * m) * PAD] = czero<V>();
             }
         } else {
 #pragma unroll
-            for (int m = 0; m < R; m++) cp_async_elem(dst + (t + R * m) * PAD, src + (size_t)(t + R * m) * N);
+            for (int m = 0; m < M; m++) cp_async_elem(dst + (t + TL * m) * PAD, src + (size_t)(t + TL * m) * N);
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
@@ -796,97 +841,96 @@ __global__ void __launch_bounds__(THREADS, 4) k_xyi_t6(Op op, int nplanes)
         __syncthreads();
         const int si = it / Op::NB, b = it % Op::NB, q = b % Op::GS, b0 = b - q;
         V *A = W + (it & 1) * PS;
-        V v[R];
-        xform<V, +1, true>(A + l * PAD, 1, t, tw, v);      // rows
-        xform<V, +1, false>(A + l, PAD, t, tw, v);         // columns: v[k2] at y = t + 6 k2
+        V v[M];
+        xform<V, S, +1, true>(A + l * PAD, 1, t, tw, v);      // rows
+        xform<V, S, +1, false>(A + l, PAD, t, tw, v);         // columns: v[m] at y = t + TL m
         if (Op::GS > 1 && q < Op::GS - 1) {
 #pragma unroll
-            for (int k2 = 0; k2 < R; k2++) keep[q][k2] = v[k2];
+            for (int m = 0; m < M; m++) keep[q][m] = v[m];
             continue;
         }
         const int item = op.item_of(tj, si);
         const bool rg = RACC && op.regacc_grid(b0);
         if (rg) {
 #pragma unroll
-            for (int k2 = 0; k2 < R; k2++) {
-                V vals[1] = {v[k2]};
-                racc[k2] = cadd(racc[k2], op.xyi_term(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals));
+            for (int m = 0; m < M; m++) {
+                V vals[1] = {v[m]};
+                racc[m] = cadd(racc[m], op.xyi_term(tj, item, b0, pz + (size_t)(t + TL * m) * N + l, vals));
                 if constexpr (Op::RACC_EXTRA)
-                    if (!sa_on) op.xyi_extra(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals);
+                    if (!sa_on) op.xyi_extra(tj, item, b0, pz + (size_t)(t + TL * m) * N + l, vals);
             }
         }
         if (sa_on) {
-            // this thread owns the accumulator points (x = l, y = t + 6 k2) of every slot;
+            // this thread owns the accumulator points (x = l, y = t + TL m) of every slot;
             // with the register form the slots hold the op's other accumulators
 #pragma unroll
-            for (int k2 = 0; k2 < R; k2++) {
+            for (int m = 0; m < M; m++) {
                 V vals[Op::GS];
 #pragma unroll
-                for (int g = 0; g < Op::GS - 1; g++) vals[g] = keep[g][k2];
-                vals[Op::GS - 1] = v[k2];
-                sacc_group(op, tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals, [&](int slot, V x) {
-                    V *a = &SAcc[(slot * N + t + R * k2) * N + l];
+                for (int g = 0; g < Op::GS - 1; g++) vals[g] = keep[g][m];
+                vals[Op::GS - 1] = v[m];
+                sacc_group(op, tj, item, b0, pz + (size_t)(t + TL * m) * N + l, vals, [&](int slot, V x) {
+                    V *a = &SAcc[(slot * N + t + TL * m) * N + l];
                     *a = cadd(*a, x);
                 });
             }
         } else if (rg) {
         } else {
 #pragma unroll
-            for (int k2 = 0; k2 < R; k2++) {
+            for (int m = 0; m < M; m++) {
                 V vals[Op::GS];
 #pragma unroll
-                for (int g = 0; g < Op::GS - 1; g++) vals[g] = keep[g][k2];
-                vals[Op::GS - 1] = v[k2];
-                op.xyi_accum(tj, item, b0, pz + (size_t)(t + R * k2) * N + l, vals);
+                for (int g = 0; g < Op::GS - 1; g++) vals[g] = keep[g][m];
+                vals[Op::GS - 1] = v[m];
+                op.xyi_accum(tj, item, b0, pz + (size_t)(t + TL * m) * N + l, vals);
             }
         }
         if (Op::REFWD && op.refwd_want(b0)) {   // uniform over the CTA
             // derived plane (orbital x density) -> forward XY FFT in place -> global
             __syncthreads();                      // the column sweep has read the set
 #pragma unroll
-            for (int k2 = 0; k2 < R; k2++) {
-                const int y = t + R * k2;
-                A[y * PAD + l] = op.refwd_load(tj, item, b0, pz + (size_t)y * N + l, v[k2]);
+            for (int m = 0; m < M; m++) {
+                const int y = t + TL * m;
+                A[y * PAD + l] = op.refwd_load(tj, item, b0, pz + (size_t)y * N + l, v[m]);
             }
             __syncthreads();
-            xform<V, -1, true>(A + l, PAD, t, tw, v);      // columns
-            xform<V, -1, true>(A + l * PAD, 1, t, tw, v);  // rows
+            xform<V, S, -1, true>(A + l, PAD, t, tw, v);      // columns
+            xform<V, S, -1, true>(A + l * PAD, 1, t, tw, v);  // rows
             V *dst = op.refwd_grid(item, b0) + pz + l;
 #pragma unroll
-            for (int m = 0; m < R; m++) dst[(size_t)(t + R * m) * N] = A[(t + R * m) * PAD + l];
+            for (int m = 0; m < M; m++) dst[(size_t)(t + TL * m) * N] = A[(t + TL * m) * PAD + l];
         }
     }
     if (RACC) {
 #pragma unroll
-        for (int k2 = 0; k2 < R; k2++) op.xyi_flush(tj, pz + (size_t)(t + R * k2) * N + l, racc[k2]);
+        for (int m = 0; m < M; m++) op.xyi_flush(tj, pz + (size_t)(t + TL * m) * N + l, racc[m]);
     }
     for (int a = 0; a < nsa; a++)
 #pragma unroll
-        for (int k2 = 0; k2 < R; k2++)
-            op.xyi_sflush(tj, a, pz + (size_t)(t + R * k2) * N + l, SAcc[(a * N + t + R * k2) * N + l]);
+        for (int m = 0; m < M; m++)
+            op.xyi_sflush(tj, a, pz + (size_t)(t + TL * m) * N + l, SAcc[(a * N + t + TL * m) * N + l]);
 }
 // shared memory of k_xyi_t6: twiddles, `sets` plane sets, `slots` FP32
 // accumulator planes (0 unless the op's SACC path is on)
-template <typename V, class Op> __host__ inline size_t smem_xyi(int sets, int slots)
+template <typename V, class Op, class S> __host__ inline size_t smem_xyi(int sets, int slots)
 {
-    return sizeof(V) * (128 + (size_t)sets * N * PAD + (sizeof(V) == 8 ? (size_t)slots * N * N : 0));
+    return sizeof(V) * (128 + (size_t)sets * S::N * S::PAD + (sizeof(V) == 8 ? (size_t)slots * S::N * S::N : 0));
 }
 
-// Z pass: one item and 32 consecutive pencils (x, y) per CTA, six threads
-// per z-line (warp t owns z = t + 6 m of all 32 pencils).  The NF inputs are
+// Z pass: one item and 32 consecutive pencils (x, y) per CTA, TL threads
+// per z-line (warp t owns z = t + TL m of all 32 pencils).  The NF inputs are
 // transformed in place in S[f][z][32]; each output is combined into O[z][32]
 // and transformed back from there.
-constexpr int ZTHREADS = R * 32;
-template <typename T, class Op>
-__global__ void __launch_bounds__(ZTHREADS, 4) k_z_t6(Op op)
+template <typename T, class Op, class S>
+__global__ void __launch_bounds__(S::ZTHREADS, S::MINB) k_z_t6(Op op)
 {
     using V = typename C2<T>::t;
-    constexpr int TC = 32;
+    constexpr int N = S::N, TL = S::TL, M = S::M, TC = 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tws = reinterpret_cast<V *>(smem_raw);
-    V *S = tws + 128;                     // [NF][N][TC]
-    V *O = S + Op::NF * N * TC;           // [N][TC]
-    const Tw<V> tw = stage<V>(op.g, tws);
+    V *Sb = tws + 128;                    // [NF][N][TC]
+    V *O = Sb + Op::NF * N * TC;          // [N][TC]
+    const Tw<V> tw = stage<V, S>(op.g, tws);
     const int item = blockIdx.y;
     const int t = threadIdx.x / TC, cl = threadIdx.x % TC;
     // pruning: the CTA takes its 32 pencils from the pair's list (active
@@ -911,58 +955,61 @@ __global__ void __launch_bounds__(ZTHREADS, 4) k_z_t6(Op op)
         const bool bl = prune && ((Op::BLI >> f) & 1);
         const V *src = op.zin_grid(item, f) + c;
 #pragma unroll
-        for (int m = 0; m < R; m++) {
-            const int z = t + R * m;
-            S[(f * N + z) * TC + cl] = (act && (!bl || pon)) ? src[(size_t)z * N * N] : czero<V>();
+        for (int m = 0; m < M; m++) {
+            const int z = t + TL * m;
+            Sb[(f * N + z) * TC + cl] = (act && (!bl || pon)) ? src[(size_t)z * N * N] : czero<V>();
         }
     }
     __syncthreads();
-    V v[R];
+    V v[M];
 #pragma unroll
     for (int f = 0; f < Op::NF; f++)
-        if (!(allin && ((Op::BLI >> f) & 1))) xform<V, -1, true>(S + f * N * TC + cl, TC, t, tw, v);
+        if (!(allin && ((Op::BLI >> f) & 1))) xform<V, S, -1, true>(Sb + f * N * TC + cl, TC, t, tw, v);
     for (int o = 0; o < Op::NB; o++) {
         const bool blo = prune && ((Op::BLO >> o) & 1);
         if (blo && allin) continue;       // uniform over the CTA
         if (Op::ZINV) __syncthreads();    // the previous output's sweep has read O
 #pragma unroll
-        for (int m = 0; m < R; m++) {
-            const int z = t + R * m;
+        for (int m = 0; m < M; m++) {
+            const int z = t + TL * m;
             V vin[Op::NF];
 #pragma unroll
-            for (int f = 0; f < Op::NF; f++) vin[f] = S[(f * N + z) * TC + cl];
+            for (int f = 0; f < Op::NF; f++) vin[f] = Sb[(f * N + z) * TC + cl];
             const V r = act ? op.zmix(item, o, x, y, z, vin) : czero<V>();
             if (Op::ZINV) O[z * TC + cl] = r;
             else if (act) op.out_grid(item, o)[c + (size_t)z * N * N] = r;   // G-space output
         }
         if (Op::ZINV) {
             __syncthreads();
-            xform<V, +1, false>(O + cl, TC, t, tw, v);   // v[k2] at z = t + 6 k2
+            xform<V, S, +1, false>(O + cl, TC, t, tw, v);   // v[m] at z = t + TL m
             if (act && (!blo || pon)) {
                 V *dst = op.out_grid(item, o) + c;
 #pragma unroll
-                for (int k2 = 0; k2 < R; k2++) dst[(size_t)(t + R * k2) * N * N] = v[k2];
+                for (int m = 0; m < M; m++) dst[(size_t)(t + TL * m) * N * N] = v[m];
             }
         }
     }
 }
-template <typename V> __host__ inline size_t smem_z(int nf) { return sizeof(V) * (128 + (size_t)(nf + 1) * N * 32); }
+template <typename V, class S> __host__ inline size_t smem_z(int nf)
+{
+    return sizeof(V) * (128 + (size_t)(nf + 1) * S::N * 32);
+}
 // Z pass with the transformed inputs kept in registers: thread (t, pencil)
 // runs stage 1 of each input's z-line straight from global memory
-// (z = t + 6 m), exchanges once through shared memory, and after stage 2
-// holds every input at z = t + 6 k2 -- the points where it evaluates the
+// (z = t + TL m), exchanges once through shared memory, and after stage 2
+// holds every input at z = t + TL m -- the points where it evaluates the
 // G-space combination of every output.  Those values are already in the
 // input order of the inverse transform's stage 1, so each output needs one
 // exchange only.  Shared memory: one exchange buffer per input.
-template <typename T, class Op>
-__global__ void __launch_bounds__(ZTHREADS, 3) k_z_t6r(Op op)
+template <typename T, class Op, class S>
+__global__ void __launch_bounds__(S::ZTHREADS, S::MINB_ZR) k_z_t6r(Op op)
 {
     using V = typename C2<T>::t;
-    constexpr int TC = 32, NF = Op::NF;
+    constexpr int N = S::N, TL = S::TL, M = S::M, TC = 32, NF = Op::NF;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tws = reinterpret_cast<V *>(smem_raw);
     V *E = tws + 128;                     // [NF][N][TC] exchange buffers
-    const Tw<V> tw = stage<V>(op.g, tws);
+    const Tw<V> tw = stage<V, S>(op.g, tws);
     const int item = blockIdx.y;
     const int t = threadIdx.x / TC, cl = threadIdx.x % TC;
     // pruning as in k_z_t6 (band-limited inputs read as zero off their support)
@@ -980,68 +1027,59 @@ __global__ void __launch_bounds__(ZTHREADS, 3) k_z_t6r(Op op)
     }
     const bool act = slot < N * N;
     const int x = c % N, y = c / N;
-    V X[NF][R];
+    V X[NF][M];
 #pragma unroll
     for (int f = 0; f < NF; f++) {
         const bool bl = prune && ((Op::BLI >> f) & 1);
         const V *src = op.zin_grid(item, f) + c;
 #pragma unroll
-        for (int m = 0; m < R; m++) X[f][m] = (act && (!bl || pon)) ? src[(size_t)(t + R * m) * N * N] : czero<V>();
+        for (int m = 0; m < M; m++) X[f][m] = (act && (!bl || pon)) ? src[(size_t)(t + TL * m) * N * N] : czero<V>();
     }
 #pragma unroll
     for (int f = 0; f < NF; f++) {
-        line_fft<V, R, -1>(X[f], tw.w6);
+        stage1<V, S, -1>(X[f], t, tw);
 #pragma unroll
-        for (int k1 = 0; k1 < R; k1++) {
-            V u = X[f][k1];
-            if (k1 > 0) u = cmul(u, tw.w[t * k1]);
-            E[(f * N + k1 * R + t) * TC + cl] = u;
-        }
+        for (int k1 = 0; k1 < M; k1++) E[(f * N + k1 * TL + t) * TC + cl] = X[f][k1];
     }
     __syncthreads();
 #pragma unroll
-    for (int f = 0; f < NF; f++) {
-#pragma unroll
-        for (int j = 0; j < R; j++) X[f][j] = E[(f * N + t * R + j) * TC + cl];
-        line_fft<V, R, -1>(X[f], tw.w6);   // X[f][k2]: input f at z = t + 6 k2
-    }
+    for (int f = 0; f < NF; f++) stage2<V, S, -1>(E + f * N * TC + cl, TC, t, tw, X[f]);   // input f at z = t + TL m
     for (int o = 0; o < Op::NB; o++) {
         const bool blo = prune && ((Op::BLO >> o) & 1);
         if (blo && allin) continue;       // uniform over the CTA
-        V v[R];
+        V v[M];
 #pragma unroll
-        for (int k2 = 0; k2 < R; k2++) {
+        for (int m = 0; m < M; m++) {
             V vin[NF];
 #pragma unroll
-            for (int f = 0; f < NF; f++) vin[f] = X[f][k2];
-            v[k2] = act ? op.zmix(item, o, x, y, t + R * k2, vin) : czero<V>();
+            for (int f = 0; f < NF; f++) vin[f] = X[f][m];
+            v[m] = act ? op.zmix(item, o, x, y, t + TL * m, vin) : czero<V>();
         }
         if (Op::ZINV) {
-            // inverse: stage 1 over m = k2 in registers, one exchange, stage 2
-            line_fft<V, R, +1>(v, tw.w6);
+            // inverse: stage 1 over m in registers, one exchange, stage 2
+            stage1<V, S, +1>(v, t, tw);
             __syncthreads();                  // the exchange buffer is free
 #pragma unroll
-            for (int k1 = 0; k1 < R; k1++) {
-                V u = v[k1];
-                if (k1 > 0) { V w = tw.w[t * k1]; w.y = -w.y; u = cmul(u, w); }
-                E[(k1 * R + t) * TC + cl] = u;
-            }
+            for (int k1 = 0; k1 < M; k1++) E[(k1 * TL + t) * TC + cl] = v[k1];
             __syncthreads();
-#pragma unroll
-            for (int j = 0; j < R; j++) v[j] = E[(t * R + j) * TC + cl];
-            line_fft<V, R, +1>(v, tw.w6);     // v[k2] at z = t + 6 k2
+            stage2<V, S, +1>(E + cl, TC, t, tw, v);   // v[m] at z = t + TL m
         }
         if (act && (!blo || pon)) {
             V *dst = op.out_grid(item, o) + c;
 #pragma unroll
-            for (int k2 = 0; k2 < R; k2++) dst[(size_t)(t + R * k2) * N * N] = v[k2];
+            for (int m = 0; m < M; m++) dst[(size_t)(t + TL * m) * N * N] = v[m];
         }
     }
 }
-template <typename V> __host__ inline size_t smem_zr(int nf) { return sizeof(V) * (128 + (size_t)nf * N * 32); }
+template <typename V, class S> __host__ inline size_t smem_zr(int nf)
+{
+    return sizeof(V) * (128 + (size_t)nf * S::N * 32);
+}
 
-
-template <typename V> __host__ inline size_t smem(int sets) { return sizeof(V) * (128 + (size_t)sets * N * PAD); }
+template <typename V, class S> __host__ inline size_t smem(int sets)
+{
+    return sizeof(V) * (128 + (size_t)sets * S::N * S::PAD);
+}
 } // namespace t6
 
 // ------------------------------------------------- XY passes, line pairs --

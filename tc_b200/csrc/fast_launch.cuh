@@ -21,15 +21,18 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
     using CP = fast::CfgP<N, sizeof(V)>;
     const bool fpair = c->xy_kernels ? c->xy_kernels == 2 : Op::XYF_PAIR;
     const bool ipair = c->xy_kernels ? c->xy_kernels == 2 : Op::XYI_PAIR;
-    // N = 36: the inverse XY pass runs with six threads per line (t6) unless a
-    // form is forced; the forward pass measured faster with one thread per
-    // line in FP32 and with t6 in FP64 (where a 36-point line spills)
-    const bool t6i = N == 36 && (c->xy_kernels == 0 || c->xy_kernels == 3);
-    const bool t6f = N == 36 && (c->xy_kernels == 3 || (c->xy_kernels == 0 && sizeof(V) == 16));
-    if constexpr (N == 36) {
+    // grids with a several-threads-per-line shape (36: 6 x 6, 48: 4 x 12):
+    // the inverse XY pass runs in that form unless another is forced; the
+    // forward pass measured faster with one thread per line in FP32 and with
+    // the split form in FP64 (where a whole line per thread spills)
+    constexpr int TLN = fast::t6::ShapeOf<N>::TL;
+    using SH = fast::t6::Shape<TLN ? N : 36, TLN ? TLN : 6>;   // (36 x 6 unused where TLN = 0)
+    const bool t6i = TLN > 0 && (c->xy_kernels == 0 || c->xy_kernels == 3);
+    const bool t6f = TLN > 0 && (c->xy_kernels == 3 || (c->xy_kernels == 0 && sizeof(V) == 16));
+    if constexpr (TLN > 0) {
         if (t6f && do_xyf)
-            TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * nf_eff * gb, fast::t6::k_xyf_t6<T, Op>,
-                              dim3(np_f), dim3(fast::t6::THREADS), fast::t6::smem<V>(1), op, np_f));
+            TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * nf_eff * gb, fast::t6::k_xyf_t6<T, Op, SH>,
+                              dim3(np_f), dim3(SH::THREADS), fast::t6::smem<V, SH>(1), op, np_f));
     }
     if (do_xyf && !t6f) {
         if (!fpair)
@@ -41,20 +44,20 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
     }
     constexpr int TC = fast::zcols<V>();
     const bool zsplit = c->z_kernels ? c->z_kernels == 2 : Op::ZSPLIT;
-    // N = 36: six threads per z-line unless a form is forced
+    // several threads per z-line unless a form is forced
     bool zt6 = false;
-    if constexpr (N == 36) {
+    if constexpr (TLN > 0) {
         zt6 = c->z_kernels == 0 || c->z_kernels == 3 || c->z_kernels == 4;
         // default: inputs transformed in place in shared memory (k_z_t6); the
         // terms with Op::ZREG keep them in registers in FP32 (k_z_t6r)
         if (c->z_kernels == 3 || (c->z_kernels == 0 && !(Op::ZREG && sizeof(V) == 8)))
             TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (nf_eff + (Op::ZINV ? nb_eff : 0)) * gb,
-                              fast::t6::k_z_t6<T, Op>, dim3((N * N + TC - 1) / TC, items), dim3(fast::t6::ZTHREADS),
-                              fast::t6::smem_z<V>(Op::NF), op));
+                              fast::t6::k_z_t6<T, Op, SH>, dim3((N * N + TC - 1) / TC, items), dim3(SH::ZTHREADS),
+                              fast::t6::smem_z<V, SH>(Op::NF), op));
         else if (zt6)
             TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (nf_eff + (Op::ZINV ? nb_eff : 0)) * gb,
-                              fast::t6::k_z_t6r<T, Op>, dim3((N * N + TC - 1) / TC, items), dim3(fast::t6::ZTHREADS),
-                              fast::t6::smem_zr<V>(Op::NF), op));
+                              fast::t6::k_z_t6r<T, Op, SH>, dim3((N * N + TC - 1) / TC, items), dim3(SH::ZTHREADS),
+                              fast::t6::smem_zr<V, SH>(Op::NF), op));
     }
     if (zt6) {
     } else if (zsplit)
@@ -65,12 +68,12 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
         TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (Op::NF + (Op::ZINV ? Op::NB : 0)) * gb,
                           fast::k_z_line<T, N, Op>, dim3((N * N + TC - 1) / TC, items), dim3(32 * fast::ZL),
                           fast::smem_z_fast<V, N>(Op::NF), op));
-    if constexpr (N == 36) {
+    if constexpr (TLN > 0) {
         if (t6i && do_xyi) {
             const int nref = Op::REFWD ? Op::NB - 1 : 0;
             return launch_tagged(c, tagname(Op::NAME, "xyi"), (double)items * (nb_eff + nref) * gb,
-                                 fast::t6::k_xyi_t6<T, Op>, dim3(np_i), dim3(fast::t6::THREADS),
-                                 fast::t6::smem_xyi<V, Op>(2, op.sacc_on ? op.sacc_n : 0) +
+                                 fast::t6::k_xyi_t6<T, Op, SH>, dim3(np_i), dim3(SH::THREADS),
+                                 fast::t6::smem_xyi<V, Op, SH>(2, op.sacc_on ? op.sacc_n : 0) +
                                      (op.m.prune ? (size_t)op.ns * sizeof(int) : 0),
                                  op, np_i);
         }

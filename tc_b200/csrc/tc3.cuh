@@ -589,12 +589,14 @@ static void op_common(tcg_ctx *c, Op &op, const ChunkPlan &p, int nsl, int ntab)
     op.m.nSB = p.nSB;
     op.m.ntab = ntab;
     op.m.nrec = c->ftab_nrec;
-    // pruning: 36^3 grid, default kernel forms (the kernels that honour it:
-    // k_xyf_fast / k_xyf_t6, k_z_t6 / k_z_t6r, k_xyi_t6), table built
+    // pruning: 36^3 or 48^3 grid, table built, split-line Z and inverse XY
+    // passes (k_z_t6 / k_z_t6r read only the active pencils, k_xyi_t6 zeroes
+    // the others; the forward XY pass may write more than the active ones)
     const int np = c->h.n[0] * c->h.n[1];
     op.m.np = np;
-    op.m.prune = (c->prune_ok && !c->no_prune && c->fast_n == 36 && !c->force_generic && c->xy_kernels == 0 &&
-                  c->z_kernels == 0 && (Op::BLI | Op::BLO) != 0) ? 1 : 0;
+    op.m.prune = (c->prune_ok && !c->no_prune && split_line_grid(c->fast_n) && !c->force_generic &&
+                  (c->xy_kernels == 0 || c->xy_kernels == 3) && (c->z_kernels == 0 || c->z_kernels >= 3) &&
+                  (Op::BLI | Op::BLO) != 0) ? 1 : 0;
     op.m.pent = p.pent;
     op.m.pfrac = op.m.prune ? p.pfrac : 1.0;
     const size_t nent = (size_t)c->h.nk * c->h.nk_all;

@@ -127,16 +127,40 @@ def test_c3_energy_vs_oracle(c3, prec):
     assert dE <= (1e-9 if prec == "fp64" else ENERGY_TOL)
 
 
+def small_n(n):
+    key = ("small", n)
+    if key not in _cache:
+        _cache[key] = synth.small("BITC", nr=(n, n, n), nk=2, ecut=2.0, nbands=2, nocc=1, seed=3)
+    return _cache[key]
+
+
 @pytest.mark.parametrize("n", [32, 40, 48])
 @pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
 def test_fast_sizes_32_40_48(n, prec, tol):
     """compile-time-size kernels of the C2, C4 and C5 grids (radix 2, 5, 3)"""
-    key = ("small", n)
-    if key not in _cache:
-        _cache[key] = synth.small("BITC", nr=(n, n, n), nk=2, ecut=2.0, nbands=2, nocc=1, seed=3)
-    s = _cache[key]
+    s = small_n(n)
     r2, r3 = oracle(s, abi.TERMS_TC)
     g2, g3 = gpu_apply(s, prec, abi.TERMS_TC)
+    assert rel(g2, r2) < tol
+    assert rel(g3, r3) < tol
+
+
+FORMS_48 = {"default": {}, "z-shared": {"z": 3}, "z-registers": {"z": 4}, "xy-split": {"xy": 3},
+            "one-thread-lines": {"xy": 1, "z": 1}, "separate-terms": {"fuse": 0}, "unpruned": {"prune": 0}}
+
+
+@pytest.mark.parametrize("form", list(FORMS_48))
+@pytest.mark.parametrize("prec,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_48_split_line_forms(form, prec, tol):
+    """48^3 (the C5 grid): the split-line kernels (four threads per line,
+    48 = 4 x 12) on pruned band-limited grids, in every kernel form, all TC
+    terms with and without shared transforms, vs the oracle"""
+    s = small_n(48)
+    r2, r3 = oracle(s, abi.TERMS_TC)
+    with Context(s, prec) as ctx:
+        ctx.set_state()
+        ctx.set_forms(**FORMS_48[form])
+        g2, g3 = ctx.apply(abi.TERMS_TC)
     assert rel(g2, r2) < tol
     assert rel(g3, r3) < tol
 
