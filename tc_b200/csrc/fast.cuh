@@ -635,7 +635,7 @@ template <int N_, int TL_> struct Shape {
     static constexpr int THREADS = TL_ * N_;     // XY passes: one plane per CTA
     static constexpr int ZTHREADS = TL_ * 32;    // Z passes: 32 pencils per CTA
     // resident CTAs per SM the launch bounds ask for (register budget)
-    static constexpr int MINB = M <= 6 ? 4 : 3;
+    static constexpr int MINB = M <= 6 ? 4 : 4;
     static constexpr int MINB_ZR = M <= 6 ? 3 : 2;
     static_assert(N_ % (TL_ * TL_) == 0, "two-stage lines need TL | N / TL");
     static_assert(N_ <= 64 && M <= 32 && TL_ <= 32, "pencil masks and twiddle slots");

@@ -28,7 +28,8 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
     constexpr int TLN = fast::t6::ShapeOf<N>::TL;
     using SH = fast::t6::Shape<TLN ? N : 36, TLN ? TLN : 6>;   // (36 x 6 unused where TLN = 0)
     const bool t6i = TLN > 0 && (c->xy_kernels == 0 || c->xy_kernels == 3);
-    const bool t6f = TLN > 0 && (c->xy_kernels == 3 || (c->xy_kernels == 0 && sizeof(V) == 16));
+    const bool t6f = TLN > 0 && (c->xy_kernels == 3 ||
+                                 (c->xy_kernels == 0 && (sizeof(V) == 16 || (N == 48 && Op::XYF_SPLIT48))));
     if constexpr (TLN > 0) {
         if (t6f && do_xyf)
             TRY(launch_tagged(c, tagname(Op::NAME, "xyf"), (double)items * nf_eff * gb, fast::t6::k_xyf_t6<T, Op, SH>,

@@ -194,6 +194,9 @@ struct OpBase {
     // 36^3 once the plane copies were made division-free) or lines split over
     // lane pairs (half the registers, one shuffle per element)
     static constexpr bool XYF_PAIR = false, XYI_PAIR = false;
+    // forward XY pass in split lines by default also in FP32 where a whole
+    // line per thread spills (48^3)
+    static constexpr bool XYF_SPLIT48 = false;
     // 36^3 Z pass: transformed inputs kept in registers (one exchange per
     // transform, fewer resident CTAs); measured faster for three inputs
     static constexpr bool ZREG = false;
@@ -673,6 +676,7 @@ struct OpTC3X : OpBase<T> {
     static constexpr const char *NAME = "3bX";
     static constexpr int NF = 3, NB = 1;
     static constexpr bool ZREG = true;
+    static constexpr bool XYF_SPLIT48 = true;    // measured faster at 48^3 (three operand grids per point)
     static constexpr bool REGACC = true;
     __device__ bool regacc_grid(int) const { return true; }
     const V *Rpsi, *Rocc, *Rchi;  // [nt][N], [ns][N], [ns][N]
