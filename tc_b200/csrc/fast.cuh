@@ -773,8 +773,11 @@ __device__ __forceinline__ void sacc_group(const Op &op, int tj, int item, int b
 // XYI: one (target, z) plane per CTA, looping over the chunk's (source,
 // output) steps; the next step's plane is copied asynchronously into the
 // second set.  GS > 1: the first GS - 1 outputs of a group wait in registers.
+// (Op::XYI_MINB_EXTRA: more resident CTAs, FP32 at 36^3, for ops that fit the
+// smaller register budget)
 template <typename T, class Op, class S>
-__global__ void __launch_bounds__(S::THREADS, S::MINB) k_xyi_t6(Op op, int nplanes)
+__global__ void __launch_bounds__(S::THREADS, S::MINB + ((S::M <= 6 && sizeof(T) == 4) ? Op::XYI_MINB_EXTRA : 0))
+    k_xyi_t6(Op op, int nplanes)
 {
     using V = typename C2<T>::t;
     constexpr int N = S::N, TL = S::TL, M = S::M, PAD = S::PAD;

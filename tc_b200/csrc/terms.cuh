@@ -197,6 +197,9 @@ struct OpBase {
     // forward XY pass in split lines by default also in FP32 where a whole
     // line per thread spills (48^3)
     static constexpr bool XYF_SPLIT48 = false;
+    // split-line inverse XY pass at 36^3: resident CTAs per SM beyond the
+    // default four (a register cap the op's work fits without spilling)
+    static constexpr int XYI_MINB_EXTRA = 0;
     // 36^3 Z pass: transformed inputs kept in registers (one exchange per
     // transform, fewer resident CTAs); measured faster for three inputs
     static constexpr bool ZREG = false;
@@ -855,6 +858,7 @@ struct OpTC2X3 : OpTC2X<T> {
     static constexpr const char *NAME = "2x3A";
     static constexpr bool REFWD = true;
     static constexpr bool RACC_EXTRA = true;
+    static constexpr int XYI_MINB_EXTRA = 1;     // 56 registers, no spills: 2x3A:xyi 638 -> 586 ms on C3
     const V *densT;               // [N] n_0 + n_1 (compute precision)
     double2 *qsum;                // [nt][3][N]
     V *tmp2;                      // [items][3][N] re-forwarded grids
