@@ -1004,8 +1004,11 @@ template <typename V, class S> __host__ inline size_t smem_z(int nf)
 // G-space combination of every output.  Those values are already in the
 // input order of the inverse transform's stage 1, so each output needs one
 // exchange only.  Shared memory: one exchange buffer per input.
+// (Op::ZR_MINB_EXTRA: more resident CTAs, FP32 at 36^3, for ops that fit the
+// smaller register budget)
 template <typename T, class Op, class S>
-__global__ void __launch_bounds__(S::ZTHREADS, S::MINB_ZR) k_z_t6r(Op op)
+__global__ void __launch_bounds__(S::ZTHREADS, S::MINB_ZR + ((S::M <= 6 && sizeof(T) == 4) ? Op::ZR_MINB_EXTRA : 0))
+    k_z_t6r(Op op)
 {
     using V = typename C2<T>::t;
     constexpr int N = S::N, TL = S::TL, M = S::M, TC = 32, NF = Op::NF;

@@ -200,6 +200,8 @@ struct OpBase {
     // split-line inverse XY pass at 36^3: resident CTAs per SM beyond the
     // default four (a register cap the op's work fits without spilling)
     static constexpr int XYI_MINB_EXTRA = 0;
+    // the same for the register-resident split-line Z pass (k_z_t6r)
+    static constexpr int ZR_MINB_EXTRA = 0;
     // 36^3 Z pass: transformed inputs kept in registers (one exchange per
     // transform, fewer resident CTAs); measured faster for three inputs
     static constexpr bool ZREG = false;
@@ -565,6 +567,7 @@ struct OpTC3B : OpBase<T> {
     using V = typename C2<T>::t;
     static constexpr const char *NAME = "3b6B";
     static constexpr bool ZREG = true;
+    static constexpr int ZR_MINB_EXTRA = EQ ? 2 : 0;   // 64 registers without spills for one spin channel
     static constexpr int NX = EQ ? 1 : 2;
     static constexpr int NF = 3 * NX, NB = 1;
     static constexpr bool REGACC = true;
@@ -680,6 +683,7 @@ struct OpTC3X : OpBase<T> {
     static constexpr int NF = 3, NB = 1;
     static constexpr bool ZREG = true;
     static constexpr bool XYF_SPLIT48 = true;    // measured faster at 48^3 (three operand grids per point)
+    static constexpr int ZR_MINB_EXTRA = 2;      // 64 registers without spills
     static constexpr bool REGACC = true;
     __device__ bool regacc_grid(int) const { return true; }
     const V *Rpsi, *Rocc, *Rchi;  // [nt][N], [ns][N], [ns][N]
