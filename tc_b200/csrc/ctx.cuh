@@ -150,6 +150,7 @@ struct tcg_ctx {
     tcg::DBuf Rpsi, Rgpsi, acc2, acc3, qsum, tmp, tmp2, aux, items, meta;
     tcg::DBuf rotw, q3b2w, nGw, Ww;           // per-state scratch kept across states (no per-step cudaMalloc / cudaFree)
     tcg::DBuf ftab;                         // mixed path: FP32 G-space coefficient records of a chunk
+    tcg::DBuf w3x;                          // [targets][3][N] compute precision: b3 dnu_d psi + b4 qsum_d (3bX input)
     int ftab_nrec = 1;
     int fast_n = 0;                         // cubic grid size with compiled fast kernels (0: generic path)
     bool force_generic = false;             // use the generic pass kernels even if fast_n is set

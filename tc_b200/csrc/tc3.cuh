@@ -61,6 +61,26 @@ __global__ void k_dot3(int N, const double2 *a, const typename C2<T>::t *b, doub
     }
 }
 
+// per-target input part of the combined 3b3 + 3b4 + 3b5 transform (OpTC3X):
+// W[t][d] = b3 dnu_d psi_t + b4 qsum[t][d], once per target instead of once
+// per (target, source) pair
+template <typename T>
+__global__ void k_w3x(int N, const typename C2<T>::t *dnu, const typename C2<T>::t *psi, const double2 *qsum,
+                      double b3, double b4, typename C2<T>::t *W, int nt)
+{
+    using V = typename C2<T>::t;
+    using S = decltype(V{}.x);
+    const size_t t = blockIdx.y;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        const V ps = psi[t * N + p];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const V w = cscale(cmul(dnu[(size_t)d * N + p], ps), (S)b3);
+            W[(t * 3 + d) * N + p] = cadd(w, cscale(from64<V>(qsum[(t * 3 + d) * N + p]), (S)b4));
+        }
+    }
+}
+
 // dnu_s[d](G) = sum_{s3} u(G; s, s3) G_d n_{s3}(G)   (tc3a1.cpp:53-70)
 static __global__ void k_dnu_g(GridDesc g, RecipC rc, Jastrow J, int s, const double2 *nG, double2 *out)
 {
@@ -1041,6 +1061,12 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
         std::vector<ChunkPlan> plan;
         TRY(plan_chunks(c, c->meta, TR.n, TR.key, TR.cartk, (int)S.key.size(), S.key, S.cartq,
                         max_items_for(c, 3, sizeof(V)), min_targets(c), plan));
+        if (acc2_fused) {   // the targets' part of the combined input, qsum now complete
+            TRY(c->w3x.ensure((size_t)TR.n * 3 * N * sizeof(V)));
+            TRY(launch(c, k_w3x<T>, dim3((unsigned)((N + 255) / 256), TR.n), dim3(256), 0, (int)N, dnuT,
+                       (const V *)(c->Rpsi.as<V>() + (size_t)TR.t0 * N), (const double2 *)(qsum + (size_t)TR.t0 * 3 * N),
+                       b3, b4, c->w3x.as<V>(), TR.n));
+        }
         for (const ChunkPlan &p : plan) {
             const size_t items = (size_t)p.nt * p.ns;
             TRY(c->tmp.ensure(items * 3 * N * sizeof(V)));
@@ -1051,13 +1077,10 @@ static int run_tc3a3b3b4b6(tcg_ctx *c, const Targets &Tg, const ApplyArgs &A, do
                 op.Rpsi = c->Rpsi.as<V>() + (size_t)(TR.t0 + p.t0) * N;
                 op.Rocc = c->Rocc.as<V>() + (S.base + p.s0) * N;
                 op.Rchi = (bitc ? c->Rchi.as<V>() : c->Rocc.as<V>()) + (S.base + p.s0) * N;
-                op.dnu = dnuT;
-                op.qsum = qsum + (size_t)(TR.t0 + p.t0) * 3 * N;
+                op.W = c->w3x.as<V>() + (size_t)p.t0 * 3 * N;
                 op.Bt = band_fused ? c->Bt.as<V>() + (S.base + p.s0) * 3 * N : nullptr;
                 op.acc = acc + (size_t)(TR.t0 + p.t0) * N;
                 op.fill = c->occfill.as<double>() + S.base + p.s0;
-                op.b3 = b3;
-                op.b4 = b4;
                 op.b5 = -band_fa4(h);
                 TRY((run_chunk<T, OpTC3X<T>>(c, op, (int)items, p.nt)));
                 continue;

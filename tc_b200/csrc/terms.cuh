@@ -687,22 +687,18 @@ struct OpTC3X : OpBase<T> {
     static constexpr bool REGACC = true;
     __device__ bool regacc_grid(int) const { return true; }
     const V *Rpsi, *Rocc, *Rchi;  // [nt][N], [ns][N], [ns][N]
-    const V *dnu;                 // [3][N] of the targets' spin
-    const double2 *qsum;          // [nt][3][N]
+    const V *W;                   // [nt][3][N] per-target part b3 dnu_d psi + b4 qsum_d (k_w3x)
     const V *Bt;                  // [ns][3][N] or null (b5 = 0)
     double2 *acc;
     const double *fill;
-    double b3, b4, b5;
+    double b5;
     __device__ V xyf_load(int item, int f, int, int, int, size_t p) const
     {
         using S = decltype(V{}.x);
         const size_t N = this->g.N;
         const int tj = item / this->ns, si = item % this->ns;
-        const V psi = __ldg(&Rpsi[(size_t)tj * N + p]);
-        V w = cscale(cmul(__ldg(&dnu[(size_t)f * N + p]), psi), (S)b3);
-        w = cadd(w, cscale(from64<V>(__ldg(&qsum[((size_t)tj * 3 + f) * N + p])), (S)b4));
-        V r = cmulc(__ldg(&Rchi[(size_t)si * N + p]), w);
-        if (Bt) r = cadd(r, cscale(cmul(__ldg(&Bt[((size_t)si * 3 + f) * N + p]), psi), (S)b5));
+        V r = cmulc(__ldg(&Rchi[(size_t)si * N + p]), __ldg(&W[((size_t)tj * 3 + f) * N + p]));
+        if (Bt) r = cadd(r, cscale(cmul(__ldg(&Bt[((size_t)si * 3 + f) * N + p]), __ldg(&Rpsi[(size_t)tj * N + p])), (S)b5));
         return r;
     }
     __device__ V zmix(int item, int, int x, int y, int z, const V *in) const
