@@ -924,15 +924,21 @@ template <typename V, class Op, class S> __host__ inline size_t smem_xyi(int set
 // per z-line (warp t owns z = t + TL m of all 32 pencils).  The NF inputs are
 // transformed in place in S[f][z][32]; each output is combined into O[z][32]
 // and transformed back from there.
+// (Op::Z_MINB_EXTRA: more resident CTAs, FP32 at 36^3, for ops that fit the
+// smaller register budget)
 template <typename T, class Op, class S>
-__global__ void __launch_bounds__(S::ZTHREADS, S::MINB) k_z_t6(Op op)
+__global__ void __launch_bounds__(S::ZTHREADS, S::MINB + ((S::M <= 6 && sizeof(T) == 4) ? Op::Z_MINB_EXTRA : 0))
+    k_z_t6(Op op)
 {
     using V = typename C2<T>::t;
     constexpr int N = S::N, TL = S::TL, M = S::M, TC = 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tws = reinterpret_cast<V *>(smem_raw);
     V *Sb = tws + 128;                    // [NF][N][TC]
-    V *O = Sb + Op::NF * N * TC;          // [N][TC]
+    // [N][TC] output plane: its own, or input plane Op::ZO_ALIAS (each thread
+    // overwrites only the points it has just read for the first output, and
+    // the later outputs read input 0 only)
+    V *O = Sb + (Op::ZO_ALIAS >= 0 ? Op::ZO_ALIAS : Op::NF) * N * TC;
     const Tw<V> tw = stage<V, S>(op.g, tws);
     const int item = blockIdx.y;
     const int t = threadIdx.x / TC, cl = threadIdx.x % TC;
@@ -993,9 +999,9 @@ __global__ void __launch_bounds__(S::ZTHREADS, S::MINB) k_z_t6(Op op)
         }
     }
 }
-template <typename V, class S> __host__ inline size_t smem_z(int nf)
+template <typename V, class S, class Op> __host__ inline size_t smem_z()
 {
-    return sizeof(V) * (128 + (size_t)(nf + 1) * S::N * 32);
+    return sizeof(V) * (128 + (size_t)(Op::NF + (Op::ZO_ALIAS >= 0 ? 0 : 1)) * S::N * 32);
 }
 // Z pass with the transformed inputs kept in registers: thread (t, pencil)
 // runs stage 1 of each input's z-line straight from global memory

@@ -54,7 +54,7 @@ int run_chunk_fast(tcg_ctx *c, const Op &op, int items, int nt, bool do_xyf, boo
         if (c->z_kernels == 3 || (c->z_kernels == 0 && !(Op::ZREG && sizeof(V) == 8)))
             TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (nf_eff + (Op::ZINV ? nb_eff : 0)) * gb,
                               fast::t6::k_z_t6<T, Op, SH>, dim3((N * N + TC - 1) / TC, items), dim3(SH::ZTHREADS),
-                              fast::t6::smem_z<V, SH>(Op::NF), op));
+                              fast::t6::smem_z<V, SH, Op>(), op));
         else if (zt6)
             TRY(launch_tagged(c, tagname(Op::NAME, "z"), (double)items * (nf_eff + (Op::ZINV ? nb_eff : 0)) * gb,
                               fast::t6::k_z_t6r<T, Op, SH>, dim3((N * N + TC - 1) / TC, items), dim3(SH::ZTHREADS),

@@ -202,6 +202,11 @@ struct OpBase {
     static constexpr int XYI_MINB_EXTRA = 0;
     // the same for the register-resident split-line Z pass (k_z_t6r)
     static constexpr int ZR_MINB_EXTRA = 0;
+    // split-line Z pass in shared memory (k_z_t6): the input plane that holds
+    // the inverse transform of each output, valid when every output after the
+    // first reads input 0 only in zmix (-1: a plane of its own)
+    static constexpr int ZO_ALIAS = -1;
+    static constexpr int Z_MINB_EXTRA = 0;    // k_z_t6 as XYI_MINB_EXTRA
     // 36^3 Z pass: transformed inputs kept in registers (one exchange per
     // transform, fewer resident CTAs); measured faster for three inputs
     static constexpr bool ZREG = false;
@@ -320,6 +325,8 @@ struct OpTC2X : OpBase<T> {
     static constexpr const char *NAME = "tc2x";
     static constexpr unsigned BLI = 0xF, BLO = 0xF;       // conj(chi_q) psi_k, conj(chi_q) grad psi_k
     static constexpr bool ZSPLIT = false;     // one thread per z-line measured faster here
+    static constexpr int ZO_ALIAS = 1;        // outputs 1-3 read input 0 only (zmix)
+    static constexpr int Z_MINB_EXTRA = 1;    // five CTAs of 38 KB at 36^3
     static constexpr bool REGACC = true;
     __device__ bool regacc_grid(int) const { return true; }
     __device__ V xyi_term(int, int item, int b, size_t p, const V *v) const
@@ -451,6 +458,7 @@ struct OpTC3A : OpBase<T> {
     static constexpr const char *NAME = "3a3b6A";
     static constexpr int NX = EQ ? 1 : 2;     // spin branches of x2 carried
     static constexpr int NF = 4, NB = 1 + 3 * NX;
+    static constexpr int ZO_ALIAS = 1;        // outputs 1.. read input 0 only (zmix)
     // input 0 = conj(chi_q) psi_k and outputs 1.. = its multiples; inputs 1-3
     // carry dnu (their products alias over the whole grid), output 0 mixes them
     static constexpr unsigned BLI = 1, BLO = ((1u << NB) - 1) & ~1u;
