@@ -207,8 +207,9 @@ struct OpBase {
     // first reads input 0 only in zmix (-1: a plane of its own)
     static constexpr int ZO_ALIAS = -1;
     static constexpr int Z_MINB_EXTRA = 0;    // k_z_t6 as XYI_MINB_EXTRA
-    // 36^3 Z pass: transformed inputs kept in registers (one exchange per
-    // transform, fewer resident CTAs); measured faster for three inputs
+    // split-line Z pass (36^3, 48^3): transformed inputs kept in registers
+    // (one exchange per transform, fewer resident CTAs); measured faster for
+    // three inputs
     static constexpr bool ZREG = false;
     GridDesc g;
     V *tmp;
@@ -239,7 +240,7 @@ struct OpBase {
     // xyi_extra(tj, item, b, p, v) (other accumulators of the op)
     static constexpr bool RACC_EXTRA = false;
     __device__ void xyi_extra(int, int, int, size_t, const V *) const {}
-    // 36^3 inverse XY pass (k_xyi_t6), FP32: SACC > 0 accumulates the chunk's
+    // split-line inverse XY pass (k_xyi_t6), FP32: SACC > 0 accumulates the chunk's
     // sources in SACC shared-memory planes per CTA (xyi_sterm picks the slot
     // of output b, -1 for none) and adds them to the FP64 accumulators once
     // at the end (xyi_sflush), instead of one FP64 red.add per source
